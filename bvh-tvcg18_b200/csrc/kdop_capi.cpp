@@ -1,0 +1,945 @@
+// kdop_capi.cpp -- the C ABI of include/kdop_cuda.h: contexts, scenes,
+// device-buffer management, statistics, CUDA-graph capture and the autotuner.
+// Kernels live in kdop_refit.cu, kdop_traverse.cu and kdop_contacts.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kdop_internal.h"
+
+using kdop::TravCtl;
+
+namespace {
+
+const int64_t kDefaultCand = 1 << 20;
+const int64_t kDefaultContacts = 1 << 20;
+const int64_t kDefaultQueue = 1 << 20;
+
+int fail(kdop_ctx* ctx, int status, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return status;
+}
+
+int cuda_fail(kdop_ctx* ctx, cudaError_t e, const char* where) {
+  std::string m = std::string(where) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();
+  return fail(ctx, KDOP_ERR_CUDA, m);
+}
+
+#define KDOP_CUDA(ctx, call)                                   \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
+  } while (0)
+
+bool valid_K(int K) { return K == 6 || K == 8 || K == 12 || K == 14 || K == 18 || K == 20 || K == 26; }
+
+template <typename T>
+cudaError_t dalloc(kdop_scene* s, T** p, int64_t n) {
+  *p = nullptr;
+  if (n <= 0) n = 1;
+  size_t bytes = (size_t)n * sizeof(T);
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e == cudaSuccess) s->device_bytes += (int64_t)bytes;
+  return e;
+}
+
+template <typename T>
+void dfree(kdop_scene* s, T** p, int64_t n) {
+  if (*p) {
+    cudaFree(*p);
+    s->device_bytes -= (int64_t)((n <= 0 ? 1 : n) * sizeof(T));
+  }
+  *p = nullptr;
+}
+
+}  // namespace
+
+namespace kdop {
+cudaError_t launch_pack3(kdop_scene* s, const float* in, float4* out, int64_t n, int with_mesh_id);
+cudaError_t launch_pack4(kdop_scene* s, const float* in, float4* out, int64_t n);
+}  // namespace kdop
+
+struct kdop_scene_ext {
+  float* stage = nullptr;
+  int64_t stage_n = 0;
+  std::vector<uint32_t> pairs_host;  // last traversed mesh pairs
+  int64_t graph_kernels = 0;
+  kdop_traverse_opts tuned{};
+  bool has_tuned = false;
+};
+
+static kdop_scene_ext* ext(kdop_scene* s);
+
+// The extension block lives right after the scene object (allocated together).
+struct SceneBox {
+  kdop_scene s;
+  kdop_scene_ext x;
+};
+static kdop_scene_ext* ext(kdop_scene* s) { return &reinterpret_cast<SceneBox*>(s)->x; }
+
+static float* stage(kdop_scene* s, int64_t nfloats, cudaError_t* err) {
+  kdop_scene_ext* x = ext(s);
+  *err = cudaSuccess;
+  if (x->stage_n < nfloats) {
+    if (x->stage) {
+      cudaFree(x->stage);
+      s->device_bytes -= x->stage_n * 4;
+    }
+    x->stage = nullptr;
+    x->stage_n = 0;
+    *err = cudaMalloc((void**)&x->stage, (size_t)std::max<int64_t>(nfloats, 1) * 4);
+    if (*err != cudaSuccess) return nullptr;
+    x->stage_n = std::max<int64_t>(nfloats, 1);
+    s->device_bytes += x->stage_n * 4;
+  }
+  return x->stage;
+}
+
+extern "C" {
+
+int kdop_api_version(void) { return KDOP_API_VERSION; }
+
+const char* kdop_status_string(int status) {
+  switch (status) {
+    case KDOP_OK: return "ok";
+    case KDOP_ERR_INVALID: return "invalid argument";
+    case KDOP_ERR_CAPACITY: return "capacity exceeded";
+    case KDOP_ERR_CUDA: return "CUDA error";
+    case KDOP_ERR_TIMEOUT: return "device wait timed out";
+    case KDOP_ERR_NOMEM: return "out of memory";
+    case KDOP_ERR_STATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+const char* kdop_last_error(const kdop_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int kdop_ctx_create(int device, kdop_ctx** out) {
+  if (!out) return KDOP_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return KDOP_ERR_CUDA;
+  }
+  if (device < 0 || device >= n) return KDOP_ERR_INVALID;
+  kdop_ctx* c = new (std::nothrow) kdop_ctx();
+  if (!c) return KDOP_ERR_NOMEM;
+  c->device = device;
+  e = cudaSetDevice(device);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+  int optin = 0;
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  c->smem_optin = (size_t)optin;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return KDOP_ERR_CUDA;
+  }
+  c->own_stream = true;
+  *out = c;
+  return KDOP_OK;
+}
+
+int kdop_ctx_destroy(kdop_ctx* ctx) {
+  if (!ctx) return KDOP_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return KDOP_OK;
+}
+
+int kdop_ctx_set_stream(kdop_ctx* ctx, void* stream) {
+  if (!ctx) return KDOP_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+  ctx->own_stream = false;
+  ctx->stream = (cudaStream_t)stream;
+  if (!stream) {
+    KDOP_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    ctx->own_stream = true;
+  }
+  return KDOP_OK;
+}
+
+void* kdop_ctx_stream(const kdop_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int kdop_ctx_synchronize(kdop_ctx* ctx) {
+  if (!ctx) return KDOP_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  KDOP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return KDOP_OK;
+}
+
+int64_t kdop_ctx_launch_count(const kdop_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+static void scene_free(kdop_scene* s) {
+  kdop_scene_ext* x = ext(s);
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->graph_exec = nullptr;
+  s->graph = nullptr;
+  dfree(s, &s->rest, s->nv);
+  dfree(s, &s->world, s->nv);
+  dfree(s, &s->tets, s->nt);
+  dfree(s, &s->surf, s->nt);
+  dfree(s, &s->nodes, s->nn * s->NW);
+  if (s->root_dev) cudaFree(s->root_dev);
+  s->root_dev = nullptr;
+  dfree(s, &s->quat, s->n_meshes);
+  dfree(s, &s->pos, s->n_meshes);
+  dfree(s, &s->lin_vel, s->n_meshes);
+  dfree(s, &s->ang_vel, s->n_meshes);
+  dfree(s, &s->phase_dev, 1);
+  dfree(s, &s->pairs, s->pairs_cap);
+  dfree(s, &s->cand, 3 * s->cand_cap);
+  dfree(s, &s->contacts, s->contact_cap);
+  dfree(s, &s->records, s->cand_cap);
+  dfree(s, &s->q_items, s->queue_cap);
+  dfree(s, &s->q_tags, s->queue_cap);
+  dfree(s, &s->ctl, 1);
+  if (s->ctl_host) cudaFreeHost(s->ctl_host);
+  s->ctl_host = nullptr;
+  if (x->stage) cudaFree(x->stage);
+  x->stage = nullptr;
+}
+
+static int grow_candidates(kdop_scene* s, int64_t n) {
+  if (n <= s->cand_cap) return KDOP_OK;
+  dfree(s, &s->cand, 3 * s->cand_cap);
+  dfree(s, &s->records, s->cand_cap);
+  s->cand_cap = 0;
+  if (n >= (int64_t)0xFFFFFFF0ll) return fail(s->ctx, KDOP_ERR_CAPACITY, "candidate capacity above 2^32");
+  KDOP_CUDA(s->ctx, dalloc(s, &s->cand, 3 * n));
+  KDOP_CUDA(s->ctx, dalloc(s, &s->records, n));
+  s->cand_cap = n;
+  return KDOP_OK;
+}
+
+static int grow_contacts(kdop_scene* s, int64_t n) {
+  if (n <= s->contact_cap) return KDOP_OK;
+  dfree(s, &s->contacts, s->contact_cap);
+  s->contact_cap = 0;
+  if (n >= (int64_t)0xFFFFFFF0ll) return fail(s->ctx, KDOP_ERR_CAPACITY, "contact capacity above 2^32");
+  KDOP_CUDA(s->ctx, dalloc(s, &s->contacts, n));
+  s->contact_cap = n;
+  return KDOP_OK;
+}
+
+static int grow_queue(kdop_scene* s, int64_t n) {
+  if (n <= s->queue_cap) return KDOP_OK;
+  dfree(s, &s->q_items, s->queue_cap);
+  dfree(s, &s->q_tags, s->queue_cap);
+  s->queue_cap = 0;
+  if (n >= (int64_t)0x7FFFFFF0ll) return fail(s->ctx, KDOP_ERR_CAPACITY, "queue capacity above 2^31");
+  KDOP_CUDA(s->ctx, dalloc(s, &s->q_items, n));
+  KDOP_CUDA(s->ctx, dalloc(s, &s->q_tags, n));
+  KDOP_CUDA(s->ctx, cudaMemsetAsync(s->q_tags, 0, (size_t)n * 4, s->ctx->stream));
+  s->queue_cap = n;
+  return KDOP_OK;
+}
+
+static int grow_pairs(kdop_scene* s, int64_t n) {
+  if (n <= s->pairs_cap) return KDOP_OK;
+  dfree(s, &s->pairs, s->pairs_cap);
+  s->pairs_cap = 0;
+  KDOP_CUDA(s->ctx, dalloc(s, &s->pairs, n));
+  s->pairs_cap = n;
+  return KDOP_OK;
+}
+
+int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* meshes, kdop_scene** out) {
+  if (!ctx || !out) return KDOP_ERR_INVALID;
+  *out = nullptr;
+  if (!valid_K(K)) return fail(ctx, KDOP_ERR_INVALID, "K must be one of 6, 8, 12, 14, 18, 20, 26");
+  if (n_meshes < 0 || (n_meshes > 0 && !meshes)) return fail(ctx, KDOP_ERR_INVALID, "bad mesh list");
+  int64_t nv = 0, nt = 0;
+  for (int m = 0; m < n_meshes; ++m) {
+    const kdop_mesh_desc& d = meshes[m];
+    if (d.n_verts < 0 || d.n_tets < 0) return fail(ctx, KDOP_ERR_INVALID, "negative mesh size");
+    if ((d.n_verts > 0 && !d.xyz) || (d.n_tets > 0 && !d.tets))
+      return fail(ctx, KDOP_ERR_INVALID, "null mesh array");
+    for (int64_t i = 0; i < 4 * d.n_tets; ++i)
+      if ((int64_t)d.tets[i] >= d.n_verts)
+        return fail(ctx, KDOP_ERR_INVALID, "tet vertex index out of range in mesh " + std::to_string(m));
+    nv += d.n_verts;
+    nt += d.n_tets;
+  }
+  if (nv >= (int64_t)0x7FFFFFFF || nt >= (int64_t)0x3FFFFFFF)
+    return fail(ctx, KDOP_ERR_INVALID, "scene too large for 32-bit indices");
+  KDOP_CUDA(ctx, cudaSetDevice(ctx->device));
+  SceneBox* box = new (std::nothrow) SceneBox();
+  if (!box) return KDOP_ERR_NOMEM;
+  kdop_scene* s = &box->s;
+  s->ctx = ctx;
+  s->K = K;
+  s->NW = (K + 2 + 3) / 4;
+  s->n_meshes = n_meshes;
+  s->nv = nv;
+  s->nt = nt;
+  s->v_off.assign((size_t)n_meshes + 1, 0);
+  s->t_off.assign((size_t)n_meshes + 1, 0);
+  for (int m = 0; m < n_meshes; ++m) {
+    s->v_off[m + 1] = s->v_off[m] + meshes[m].n_verts;
+    s->t_off[m + 1] = s->t_off[m] + meshes[m].n_tets;
+  }
+  std::memset(&s->dirs, 0, sizeof(s->dirs));
+  kdop::direction_table(K, &s->dirs.d[0][0]);
+
+  // host tree build
+  std::vector<const float*> xyz((size_t)n_meshes);
+  std::vector<const uint32_t*> tets((size_t)n_meshes);
+  std::vector<int64_t> nvs((size_t)n_meshes), nts((size_t)n_meshes);
+  for (int m = 0; m < n_meshes; ++m) {
+    xyz[m] = meshes[m].xyz;
+    tets[m] = meshes[m].tets;
+    nvs[m] = meshes[m].n_verts;
+    nts[m] = meshes[m].n_tets;
+  }
+  kdop::ForestBuild fb;
+  if (kdop::build_forest(xyz, nvs, tets, nts, s->t_off, fb) != 0) {
+    delete box;
+    return fail(ctx, KDOP_ERR_INVALID, "scene too large for 31-bit node indices");
+  }
+  s->level_off = fb.level_off;
+  s->root = fb.root;
+  s->nn = fb.level_off.empty() ? 0 : fb.level_off.back();
+  s->depth = fb.depth;
+
+  // host staging of meshes
+  std::vector<float4> rest((size_t)std::max<int64_t>(nv, 1));
+  std::vector<uint4> gt((size_t)std::max<int64_t>(nt, 1));
+  std::vector<uint8_t> surf((size_t)std::max<int64_t>(nt, 1));
+  for (int m = 0; m < n_meshes; ++m) {
+    const kdop_mesh_desc& d = meshes[m];
+    int mid = m;
+    float midf;
+    std::memcpy(&midf, &mid, 4);
+    for (int64_t i = 0; i < d.n_verts; ++i)
+      rest[s->v_off[m] + i] = make_float4(d.xyz[3 * i], d.xyz[3 * i + 1], d.xyz[3 * i + 2], midf);
+    uint32_t vo = (uint32_t)s->v_off[m];
+    for (int64_t t = 0; t < d.n_tets; ++t)
+      gt[s->t_off[m] + t] = make_uint4(d.tets[4 * t] + vo, d.tets[4 * t + 1] + vo, d.tets[4 * t + 2] + vo,
+                                       d.tets[4 * t + 3] + vo);
+    if (d.surface)
+      std::memcpy(&surf[s->t_off[m]], d.surface, (size_t)d.n_tets);
+    else if (d.n_tets)
+      kdop::surface_map(d.n_tets, d.tets, &surf[s->t_off[m]]);
+  }
+
+  int rc = KDOP_OK;
+  cudaStream_t st = ctx->stream;
+  uint32_t* topo_dev = nullptr;
+  do {
+    cudaError_t e;
+#define SC_TRY(call)                                 \
+  if ((e = (call)) != cudaSuccess) {                 \
+    rc = cuda_fail(ctx, e, #call);                   \
+    break;                                           \
+  }
+    SC_TRY(dalloc(s, &s->rest, nv));
+    SC_TRY(dalloc(s, &s->world, nv));
+    SC_TRY(dalloc(s, &s->tets, nt));
+    SC_TRY(dalloc(s, &s->surf, nt));
+    SC_TRY(dalloc(s, &s->nodes, s->nn * s->NW));
+    size_t root_words = (size_t)((n_meshes + 1) & ~1);
+    size_t root_bytes = root_words * 4 + s->level_off.size() * 8;
+    SC_TRY(cudaMalloc((void**)&s->root_dev, std::max<size_t>(root_bytes, 8)));
+    s->device_bytes += (int64_t)root_bytes;
+    SC_TRY(dalloc(s, &s->quat, n_meshes));
+    SC_TRY(dalloc(s, &s->pos, n_meshes));
+    SC_TRY(dalloc(s, &s->lin_vel, n_meshes));
+    SC_TRY(dalloc(s, &s->ang_vel, n_meshes));
+    SC_TRY(dalloc(s, &s->phase_dev, 1));
+    SC_TRY(dalloc(s, &s->ctl, 1));
+    SC_TRY(cudaMallocHost((void**)&s->ctl_host, sizeof(TravCtl)));
+    std::memset(s->ctl_host, 0, sizeof(TravCtl));
+    SC_TRY(cudaMemcpyAsync(s->rest, rest.data(), (size_t)nv * sizeof(float4), cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMemcpyAsync(s->world, rest.data(), (size_t)nv * sizeof(float4), cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMemcpyAsync(s->tets, gt.data(), (size_t)nt * sizeof(uint4), cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMemcpyAsync(s->surf, surf.data(), (size_t)nt, cudaMemcpyHostToDevice, st));
+    std::vector<uint8_t> rbuf(std::max<size_t>(root_bytes, 8), 0);
+    if (n_meshes) std::memcpy(rbuf.data(), s->root.data(), (size_t)n_meshes * 4);
+    if (!s->level_off.empty()) std::memcpy(rbuf.data() + root_words * 4, s->level_off.data(), s->level_off.size() * 8);
+    SC_TRY(cudaMemcpyAsync(s->root_dev, rbuf.data(), root_bytes, cudaMemcpyHostToDevice, st));
+    std::vector<float4> q((size_t)std::max(n_meshes, 1), make_float4(1.f, 0.f, 0.f, 0.f));
+    std::vector<float4> z((size_t)std::max(n_meshes, 1), make_float4(0.f, 0.f, 0.f, 0.f));
+    SC_TRY(cudaMemcpyAsync(s->quat, q.data(), (size_t)n_meshes * sizeof(float4), cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMemcpyAsync(s->pos, z.data(), (size_t)n_meshes * sizeof(float4), cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMemcpyAsync(s->lin_vel, z.data(), (size_t)n_meshes * sizeof(float4), cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMemcpyAsync(s->ang_vel, z.data(), (size_t)n_meshes * sizeof(float4), cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMemsetAsync(s->phase_dev, 0, sizeof(float), st));
+    SC_TRY(cudaMemsetAsync(s->ctl, 0, sizeof(TravCtl), st));
+    SC_TRY(cudaMalloc((void**)&topo_dev, std::max<size_t>(fb.topo.size(), 1) * 4));
+    SC_TRY(cudaMemcpyAsync(topo_dev, fb.topo.data(), fb.topo.size() * 4, cudaMemcpyHostToDevice, st));
+    SC_TRY(kdop::launch_write_topology(s, topo_dev));
+    // make_tree ends with a refit (kdop_make_tree.h:285)
+    SC_TRY(kdop::launch_refit(s, KDOP_REFIT_VERTICES));
+    s->refit_mode = KDOP_REFIT_VERTICES;
+    s->have_world = true;
+    SC_TRY(cudaStreamSynchronize(st));
+#undef SC_TRY
+  } while (0);
+  if (topo_dev) cudaFree(topo_dev);
+  if (rc == KDOP_OK) rc = grow_candidates(s, kDefaultCand);
+  if (rc == KDOP_OK) rc = grow_contacts(s, kDefaultContacts);
+  if (rc == KDOP_OK) rc = grow_queue(s, kDefaultQueue);
+  if (rc == KDOP_OK) rc = grow_pairs(s, std::max(n_meshes, 1));
+  if (rc != KDOP_OK) {
+    scene_free(s);
+    delete box;
+    return rc;
+  }
+  *out = s;
+  return KDOP_OK;
+}
+
+int kdop_scene_destroy(kdop_scene* s) {
+  if (!s) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  scene_free(s);
+  delete reinterpret_cast<SceneBox*>(s);
+  return KDOP_OK;
+}
+
+int kdop_scene_get_info(const kdop_scene* s, kdop_scene_info* info) {
+  if (!s || !info) return KDOP_ERR_INVALID;
+  info->K = s->K;
+  info->n_meshes = s->n_meshes;
+  info->n_verts = s->nv;
+  info->n_tets = s->nt;
+  info->n_nodes = s->nn;
+  info->depth = s->depth;
+  info->node_bytes = s->NW * 16;
+  info->device_bytes = s->device_bytes;
+  return KDOP_OK;
+}
+
+int kdop_read_tree(kdop_scene* s, int mesh, int64_t cap, float* vol, int64_t* tet, int64_t* n_nodes) {
+  if (!s || mesh < 0 || mesh >= s->n_meshes || !n_nodes) return KDOP_ERR_INVALID;
+  int64_t ntm = s->t_off[mesh + 1] - s->t_off[mesh];
+  *n_nodes = ntm > 0 ? 2 * ntm - 1 : 0;
+  if (*n_nodes == 0) return KDOP_OK;
+  if (cap < *n_nodes) return fail(s->ctx, KDOP_ERR_CAPACITY, "tree read buffer too small");
+  if (!vol || !tet) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  std::vector<float> rec((size_t)(s->nn * s->NW * 4));
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(rec.data(), s->nodes, rec.size() * 4, cudaMemcpyDeviceToHost, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  const int W = s->NW * 4;
+  const int tw = s->K;  // word index of `start`
+  std::vector<uint32_t> stack(1, s->root[mesh]);
+  int64_t k = 0;
+  while (!stack.empty()) {
+    uint32_t n = stack.back();
+    stack.pop_back();
+    const float* r = &rec[(size_t)n * W];
+    uint32_t st, en;
+    std::memcpy(&st, r + tw, 4);
+    std::memcpy(&en, r + tw + 1, 4);
+    if (k >= *n_nodes) return fail(s->ctx, KDOP_ERR_STATE, "tree walk overran the node count");
+    std::memcpy(vol + k * s->K, r, (size_t)s->K * 4);
+    if (st == en) {
+      tet[k] = (int64_t)st - s->t_off[mesh];
+    } else {
+      tet[k] = -1;
+      stack.push_back(en);
+      stack.push_back(st);
+    }
+    ++k;
+  }
+  return KDOP_OK;
+}
+
+int kdop_set_vertices(kdop_scene* s, const float* xyz, int64_t n, int memory) {
+  if (!s || (n > 0 && !xyz) || n != s->nv) return s ? fail(s->ctx, KDOP_ERR_INVALID, "vertex count mismatch") : KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  if (n == 0) return KDOP_OK;
+  const float* src = xyz;
+  if (memory == KDOP_HOST) {
+    cudaError_t e;
+    float* d = stage(s, 3 * n, &e);
+    if (!d) return cuda_fail(s->ctx, e, "staging alloc");
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(d, xyz, (size_t)n * 12, cudaMemcpyHostToDevice, s->ctx->stream));
+    src = d;
+  }
+  KDOP_CUDA(s->ctx, kdop::launch_pack3(s, src, s->world, n, 0));
+  s->have_world = true;
+  return KDOP_OK;
+}
+
+int kdop_set_poses(kdop_scene* s, const float* quat, const float* pos, int memory) {
+  if (!s || (s->n_meshes > 0 && (!quat || !pos))) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  int64_t n = s->n_meshes;
+  if (n == 0) return KDOP_OK;
+  const float* q = quat;
+  const float* p = pos;
+  if (memory == KDOP_HOST) {
+    cudaError_t e;
+    float* d = stage(s, 7 * n, &e);
+    if (!d) return cuda_fail(s->ctx, e, "staging alloc");
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(d, quat, (size_t)n * 16, cudaMemcpyHostToDevice, s->ctx->stream));
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(d + 4 * n, pos, (size_t)n * 12, cudaMemcpyHostToDevice, s->ctx->stream));
+    q = d;
+    p = d + 4 * n;
+  }
+  KDOP_CUDA(s->ctx, kdop::launch_pack4(s, q, s->quat, n));
+  KDOP_CUDA(s->ctx, kdop::launch_pack3(s, p, s->pos, n, -1));
+  return KDOP_OK;
+}
+
+int kdop_set_deformation(kdop_scene* s, float amp, float w, float phase) {
+  if (!s) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  s->amp = amp;
+  s->w = w;
+  s->phase = phase;
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->phase_dev, &s->phase, 4, cudaMemcpyHostToDevice, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  return KDOP_OK;
+}
+
+int kdop_set_motion(kdop_scene* s, const float* lin, const float* ang, float phase_rate, int memory) {
+  if (!s || (s->n_meshes > 0 && (!lin || !ang))) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  int64_t n = s->n_meshes;
+  s->phase_rate = phase_rate;
+  if (n == 0) return KDOP_OK;
+  const float* l = lin;
+  const float* a = ang;
+  if (memory == KDOP_HOST) {
+    cudaError_t e;
+    float* d = stage(s, 6 * n, &e);
+    if (!d) return cuda_fail(s->ctx, e, "staging alloc");
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(d, lin, (size_t)n * 12, cudaMemcpyHostToDevice, s->ctx->stream));
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(d + 3 * n, ang, (size_t)n * 12, cudaMemcpyHostToDevice, s->ctx->stream));
+    l = d;
+    a = d + 3 * n;
+  }
+  KDOP_CUDA(s->ctx, kdop::launch_pack3(s, l, s->lin_vel, n, -1));
+  KDOP_CUDA(s->ctx, kdop::launch_pack3(s, a, s->ang_vel, n, -1));
+  return KDOP_OK;
+}
+
+int kdop_refit(kdop_scene* s, int mode) {
+  if (!s) return KDOP_ERR_INVALID;
+  if (mode < KDOP_REFIT_VERTICES || mode > KDOP_REFIT_DEFORM) return fail(s->ctx, KDOP_ERR_INVALID, "bad refit mode");
+  cudaSetDevice(s->ctx->device);
+  s->refit_mode = mode;
+  KDOP_CUDA(s->ctx, kdop::launch_refit(s, mode));
+  return KDOP_OK;
+}
+
+int kdop_read_vertices(kdop_scene* s, float* xyz, int64_t cap) {
+  if (!s || cap < s->nv || (s->nv > 0 && !xyz)) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  if (s->nv == 0) return KDOP_OK;
+  std::vector<float4> h((size_t)s->nv);
+  float4* src = s->world;
+  float4* tmp = nullptr;
+  int mode = s->refit_mode < 0 ? 0 : s->refit_mode;
+  if (mode != KDOP_REFIT_VERTICES) {
+    KDOP_CUDA(s->ctx, cudaMalloc((void**)&tmp, (size_t)s->nv * sizeof(float4)));
+    cudaError_t e = kdop::launch_world(s, mode, tmp);
+    if (e != cudaSuccess) {
+      cudaFree(tmp);
+      return cuda_fail(s->ctx, e, "launch_world");
+    }
+    src = tmp;
+  }
+  cudaError_t e = cudaMemcpyAsync(h.data(), src, (size_t)s->nv * sizeof(float4), cudaMemcpyDeviceToHost, s->ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->ctx->stream);
+  if (tmp) cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "read vertices");
+  for (int64_t i = 0; i < s->nv; ++i) {
+    xyz[3 * i] = h[i].x;
+    xyz[3 * i + 1] = h[i].y;
+    xyz[3 * i + 2] = h[i].z;
+  }
+  return KDOP_OK;
+}
+
+static int resolve_opts(const kdop_scene* s, const kdop_traverse_opts* o, kdop::TravParams& p, int& mode) {
+  kdop_traverse_opts d;
+  kdop_traverse_opts_default(s, &d);
+  if (!o) o = &d;
+  mode = o->mode;
+  if (mode != KDOP_TRAVERSE_BATCHED && mode != KDOP_TRAVERSE_PLAIN) return KDOP_ERR_INVALID;
+  p.block_warps = o->block_warps > 0 ? o->block_warps : d.block_warps;
+  p.stack_cap = o->stack_cap > 0 ? o->stack_cap : d.stack_cap;
+  p.init_chunk = o->init_chunk > 0 ? o->init_chunk : d.init_chunk;
+  p.donate_min = o->donate_min > 0 ? o->donate_min : d.donate_min;
+  p.timeout_ns = (long long)(o->timeout_ms > 0 ? o->timeout_ms : 5000) * 1000000ll;
+  p.surface_filter = o->surface_filter ? 1 : 0;
+  if (p.block_warps > 16 || (p.stack_cap & (p.stack_cap - 1)) || p.stack_cap < 64 || p.init_chunk > 32)
+    return KDOP_ERR_INVALID;
+  if (kdop::traverse_smem_bytes(p.block_warps, p.stack_cap) > s->ctx->smem_optin) return KDOP_ERR_INVALID;
+  return KDOP_OK;
+}
+
+int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
+  if (!o) return KDOP_ERR_INVALID;
+  std::memset(o, 0, sizeof(*o));
+  o->mode = KDOP_TRAVERSE_BATCHED;
+  o->surface_filter = 1;
+  o->block_warps = 8;
+  o->stack_cap = 512;
+  o->init_chunk = 1;
+  o->donate_min = 64;
+  o->timeout_ms = 5000;
+  if (s) {
+    kdop_scene_ext* x = ext(const_cast<kdop_scene*>(s));
+    if (x->has_tuned) {
+      o->block_warps = x->tuned.block_warps;
+      o->stack_cap = x->tuned.stack_cap;
+      o->init_chunk = x->tuned.init_chunk;
+      o->donate_min = x->tuned.donate_min;
+    }
+  }
+  return KDOP_OK;
+}
+
+static int upload_pairs(kdop_scene* s, int64_t n, const uint32_t* pairs, int memory) {
+  kdop_scene_ext* x = ext(s);
+  int rc = grow_pairs(s, std::max<int64_t>(n, 1));
+  if (rc != KDOP_OK) return rc;
+  if (n == 0) {
+    x->pairs_host.clear();
+    return KDOP_OK;
+  }
+  if (memory == KDOP_HOST) {
+    for (int64_t i = 0; i < 2 * n; ++i)
+      if ((int64_t)pairs[i] >= s->n_meshes) return fail(s->ctx, KDOP_ERR_INVALID, "mesh index out of range in pairs");
+    x->pairs_host.assign(pairs, pairs + 2 * n);
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->pairs, pairs, (size_t)n * 8, cudaMemcpyHostToDevice, s->ctx->stream));
+  } else {
+    x->pairs_host.assign((size_t)(2 * n), 0);
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(x->pairs_host.data(), pairs, (size_t)n * 8, cudaMemcpyDeviceToHost,
+                                      s->ctx->stream));
+    KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    for (int64_t i = 0; i < 2 * n; ++i)
+      if ((int64_t)x->pairs_host[i] >= s->n_meshes)
+        return fail(s->ctx, KDOP_ERR_INVALID, "mesh index out of range in pairs");
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->pairs, pairs, (size_t)n * 8, cudaMemcpyDeviceToDevice, s->ctx->stream));
+  }
+  return KDOP_OK;
+}
+
+int kdop_traverse(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int memory, const kdop_traverse_opts* opts) {
+  if (!s || n_pairs < 0 || (n_pairs > 0 && !pairs)) return KDOP_ERR_INVALID;
+  if (n_pairs >= (int64_t)0x7FFFFFFF) return fail(s->ctx, KDOP_ERR_INVALID, "too many pairs");
+  cudaSetDevice(s->ctx->device);
+  kdop::TravParams p;
+  int mode = 0;
+  if (resolve_opts(s, opts, p, mode) != KDOP_OK) return fail(s->ctx, KDOP_ERR_INVALID, "bad traversal options");
+  int rc = upload_pairs(s, n_pairs, pairs, memory);
+  if (rc != KDOP_OK) return rc;
+  KDOP_CUDA(s->ctx, kdop::launch_traverse(s, n_pairs, s->pairs, p, mode == KDOP_TRAVERSE_PLAIN));
+  s->traversed = true;
+  s->contacted = false;
+  s->last_pairs = n_pairs;
+  s->last_mode = mode;
+  s->last_params = p;
+  return KDOP_OK;
+}
+
+int kdop_get_stats(kdop_scene* s, kdop_stats* st) {
+  if (!s || !st) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  const TravCtl& c = *s->ctl_host;
+  std::memset(st, 0, sizeof(*st));
+  st->n_pairs = s->last_pairs;
+  st->n_tests = (int64_t)c.tests;
+  st->n_leaf_overlaps = (int64_t)c.leaf_overlaps;
+  st->n_candidates = (int64_t)c.n_cand;
+  st->n_contacts = s->contacted ? (int64_t)c.n_contacts : 0;
+  st->candidate_capacity = s->cand_cap;
+  st->contact_capacity = s->contact_cap;
+  st->queue_capacity = s->queue_cap;
+  st->queue_used = (int64_t)c.q_tail;
+  st->device_error = (int32_t)c.error;
+  if (c.error & (kdop::DEV_ERR_TIMEOUT | kdop::DEV_ERR_QUEUE_FULL)) {
+    // leave the queue clean for the next launch
+    KDOP_CUDA(s->ctx, cudaMemsetAsync(s->q_tags, 0, (size_t)s->queue_cap * 4, s->ctx->stream));
+    KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  }
+  if (c.error & kdop::DEV_ERR_TIMEOUT) return fail(s->ctx, KDOP_ERR_TIMEOUT, "traversal wait timed out");
+  if (c.error & kdop::DEV_ERR_QUEUE_FULL) return fail(s->ctx, KDOP_ERR_CAPACITY, "traversal work queue full");
+  if (c.error & kdop::DEV_ERR_BAD_INDEX) return fail(s->ctx, KDOP_ERR_INVALID, "bad index on device");
+  if ((int64_t)c.n_cand > s->cand_cap) return fail(s->ctx, KDOP_ERR_CAPACITY, "candidate buffer full");
+  if (s->contacted && (int64_t)c.n_contacts > s->contact_cap)
+    return fail(s->ctx, KDOP_ERR_CAPACITY, "contact buffer full");
+  return KDOP_OK;
+}
+
+int kdop_reserve(kdop_scene* s, int64_t candidates, int64_t contacts, int64_t queue) {
+  if (!s || candidates < 0 || contacts < 0 || queue < 0) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  int rc = KDOP_OK;
+  if (candidates) rc = grow_candidates(s, candidates);
+  if (rc == KDOP_OK && contacts) rc = grow_contacts(s, contacts);
+  if (rc == KDOP_OK && queue) rc = grow_queue(s, queue);
+  if (rc == KDOP_OK) KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  return rc;
+}
+
+int kdop_set_capacity(kdop_scene* s, int64_t candidates, int64_t contacts, int64_t queue) {
+  if (!s || candidates < 0 || contacts < 0 || queue < 0) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  int rc = KDOP_OK;
+  if (candidates) {
+    dfree(s, &s->cand, 3 * s->cand_cap);
+    dfree(s, &s->records, s->cand_cap);
+    s->cand_cap = 0;
+    rc = grow_candidates(s, candidates);
+  }
+  if (rc == KDOP_OK && contacts) {
+    dfree(s, &s->contacts, s->contact_cap);
+    s->contact_cap = 0;
+    rc = grow_contacts(s, contacts);
+  }
+  if (rc == KDOP_OK && queue) {
+    dfree(s, &s->q_items, s->queue_cap);
+    dfree(s, &s->q_tags, s->queue_cap);
+    s->queue_cap = 0;
+    rc = grow_queue(s, queue);
+  }
+  s->traversed = s->contacted = false;
+  if (rc == KDOP_OK) KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  return rc;
+}
+
+int kdop_read_candidates(kdop_scene* s, uint32_t* rows, int64_t cap, int64_t* n_rows) {
+  if (!s || !n_rows || (cap > 0 && !rows)) return KDOP_ERR_INVALID;
+  if (!s->traversed) return fail(s->ctx, KDOP_ERR_STATE, "no traversal yet");
+  cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  int64_t n = std::min<int64_t>((int64_t)s->ctl_host->n_cand, s->cand_cap);
+  *n_rows = n;
+  if (n > cap) return fail(s->ctx, KDOP_ERR_CAPACITY, "candidate read buffer too small");
+  if (n == 0) return KDOP_OK;
+  std::vector<uint32_t> h(3 * (size_t)n);
+  for (int k = 0; k < 3; ++k)
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(h.data() + k * n, s->cand + k * s->cand_cap, (size_t)n * 4,
+                                      cudaMemcpyDeviceToHost, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  const std::vector<uint32_t>& ph = ext(s)->pairs_host;
+  for (int64_t i = 0; i < n; ++i) {
+    uint32_t p = h[2 * n + i];
+    uint32_t ma = ph[2 * p], mb = ph[2 * p + 1];
+    rows[3 * i] = p;
+    rows[3 * i + 1] = (uint32_t)((int64_t)h[i] - s->t_off[ma]);
+    rows[3 * i + 2] = (uint32_t)((int64_t)h[n + i] - s->t_off[mb]);
+  }
+  return KDOP_OK;
+}
+
+int kdop_contacts(kdop_scene* s) {
+  if (!s) return KDOP_ERR_INVALID;
+  if (!s->traversed) return fail(s->ctx, KDOP_ERR_STATE, "kdop_contacts before kdop_traverse");
+  cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, kdop::launch_contacts(s));
+  s->contacted = true;
+  return KDOP_OK;
+}
+
+int kdop_read_contacts(kdop_scene* s, kdop_contact* rows, int64_t cap, int64_t* n_rows) {
+  if (!s || !n_rows || (cap > 0 && !rows)) return KDOP_ERR_INVALID;
+  if (!s->contacted) return fail(s->ctx, KDOP_ERR_STATE, "no contacts yet");
+  cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  int64_t n = std::min<int64_t>((int64_t)s->ctl_host->n_contacts, s->contact_cap);
+  *n_rows = n;
+  if (n > cap) return fail(s->ctx, KDOP_ERR_CAPACITY, "contact read buffer too small");
+  if (n == 0) return KDOP_OK;
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(rows, s->contacts, (size_t)n * sizeof(kdop_contact), cudaMemcpyDeviceToHost,
+                                    s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  return KDOP_OK;
+}
+
+int kdop_contacts_adjoint(kdop_scene* s, const float* dd, const float* dn, float* grad, int memory) {
+  if (!s || !dd || !grad) return KDOP_ERR_INVALID;
+  if (!s->contacted) return fail(s->ctx, KDOP_ERR_STATE, "adjoint before kdop_contacts");
+  cudaSetDevice(s->ctx->device);
+  if (memory == KDOP_DEVICE) {
+    KDOP_CUDA(s->ctx, kdop::launch_adjoint(s, dd, dn, grad));
+    return KDOP_OK;
+  }
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->ctl_host, s->ctl, sizeof(TravCtl), cudaMemcpyDeviceToHost, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  int64_t nc = std::min<int64_t>((int64_t)s->ctl_host->n_contacts, s->contact_cap);
+  int64_t need = std::max<int64_t>(nc, 1) * 4 + 3 * s->nv;
+  cudaError_t e;
+  float* d = stage(s, need, &e);
+  if (!d) return cuda_fail(s->ctx, e, "staging alloc");
+  float* d_dd = d;
+  float* d_dn = d + std::max<int64_t>(nc, 1);
+  float* d_g = d + 4 * std::max<int64_t>(nc, 1);
+  if (nc) KDOP_CUDA(s->ctx, cudaMemcpyAsync(d_dd, dd, (size_t)nc * 4, cudaMemcpyHostToDevice, s->ctx->stream));
+  if (nc && dn) KDOP_CUDA(s->ctx, cudaMemcpyAsync(d_dn, dn, (size_t)nc * 12, cudaMemcpyHostToDevice, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(d_g, grad, (size_t)s->nv * 12, cudaMemcpyHostToDevice, s->ctx->stream));
+  KDOP_CUDA(s->ctx, kdop::launch_adjoint(s, d_dd, dn ? d_dn : nullptr, d_g));
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(grad, d_g, (size_t)s->nv * 12, cudaMemcpyDeviceToHost, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  return KDOP_OK;
+}
+
+int kdop_graph_release(kdop_scene* s) {
+  if (!s) return KDOP_ERR_INVALID;
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->graph_exec = nullptr;
+  s->graph = nullptr;
+  ext(s)->graph_kernels = 0;
+  return KDOP_OK;
+}
+
+int kdop_graph_capture(kdop_scene* s, int refit_mode, int64_t n_pairs, const uint32_t* pairs, int memory,
+                       const kdop_traverse_opts* opts, int flags) {
+  if (!s || n_pairs < 0 || (n_pairs > 0 && !pairs)) return KDOP_ERR_INVALID;
+  if (refit_mode < KDOP_REFIT_VERTICES || refit_mode > KDOP_REFIT_DEFORM) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  kdop::TravParams p;
+  int mode = 0;
+  if (resolve_opts(s, opts, p, mode) != KDOP_OK) return fail(s->ctx, KDOP_ERR_INVALID, "bad traversal options");
+  kdop_graph_release(s);
+  int rc = upload_pairs(s, n_pairs, pairs, memory);
+  if (rc != KDOP_OK) return rc;
+  // settle function attributes outside the capture
+  KDOP_CUDA(s->ctx, kdop::traverse_prepare(s->K, kdop::traverse_smem_bytes(p.block_warps, p.stack_cap)));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+  long long before = s->ctx->launches;
+  KDOP_CUDA(s->ctx, cudaStreamBeginCapture(s->ctx->stream, cudaStreamCaptureModeRelaxed));
+  cudaError_t e = cudaSuccess;
+  if (flags & 1) e = kdop::launch_motion(s);
+  if (e == cudaSuccess) e = kdop::launch_refit(s, refit_mode);
+  if (e == cudaSuccess) e = kdop::launch_traverse(s, n_pairs, s->pairs, p, mode == KDOP_TRAVERSE_PLAIN);
+  if (e == cudaSuccess) e = kdop::launch_contacts(s);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(s->ctx->stream, &g);
+  s->ctx->launches = before;
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    return cuda_fail(s->ctx, e != cudaSuccess ? e : e2, "graph capture");
+  }
+  s->graph = g;
+  e = cudaGraphInstantiate(&s->graph_exec, g, 0);
+  if (e != cudaSuccess) {
+    kdop_graph_release(s);
+    return cuda_fail(s->ctx, e, "cudaGraphInstantiate");
+  }
+  size_t n_nodes = 0;
+  cudaGraphGetNodes(g, nullptr, &n_nodes);
+  ext(s)->graph_kernels = (int64_t)n_nodes;
+  s->refit_mode = refit_mode;
+  s->traversed = true;
+  s->contacted = true;
+  s->last_pairs = n_pairs;
+  s->last_mode = mode;
+  s->last_params = p;
+  return KDOP_OK;
+}
+
+int kdop_graph_launch(kdop_scene* s) {
+  if (!s) return KDOP_ERR_INVALID;
+  if (!s->graph_exec) return fail(s->ctx, KDOP_ERR_STATE, "no captured graph");
+  cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, cudaGraphLaunch(s->graph_exec, s->ctx->stream));
+  s->ctx->launches += ext(s)->graph_kernels;
+  return KDOP_OK;
+}
+
+int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int memory, int repeats,
+                  kdop_traverse_opts* best) {
+  if (!s || n_pairs < 0 || (n_pairs > 0 && !pairs)) return KDOP_ERR_INVALID;
+  cudaSetDevice(s->ctx->device);
+  if (repeats < 1) repeats = 1;
+  int rc = upload_pairs(s, n_pairs, pairs, memory);
+  if (rc != KDOP_OK) return rc;
+  const int warps[] = {4, 8, 16};
+  const int caps[] = {256, 512, 1024};
+  const int chunks[] = {1, 4};
+  const int donate[] = {32, 96};
+  cudaEvent_t e0, e1;
+  KDOP_CUDA(s->ctx, cudaEventCreate(&e0));
+  KDOP_CUDA(s->ctx, cudaEventCreate(&e1));
+  float best_ms = 1e30f;
+  kdop_traverse_opts bo;
+  kdop_traverse_opts_default(nullptr, &bo);
+  for (int w : warps)
+    for (int c : caps)
+      for (int ch : chunks)
+        for (int dm : donate) {
+          kdop::TravParams p;
+          p.block_warps = w;
+          p.stack_cap = c;
+          p.init_chunk = ch;
+          p.donate_min = dm;
+          p.timeout_ns = 5000000000ll;
+          p.surface_filter = 1;
+          if (kdop::traverse_smem_bytes(w, c) > s->ctx->smem_optin) continue;
+          // warm-up run, also checks the buffers are large enough
+          cudaError_t e = kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
+          if (e != cudaSuccess) continue;
+          kdop_stats st;
+          int r = kdop_get_stats(s, &st);
+          if (r == KDOP_ERR_CAPACITY) {
+            int64_t nc = std::max<int64_t>(st.n_candidates + st.n_candidates / 4, s->cand_cap);
+            int64_t nq = (st.device_error & kdop::DEV_ERR_QUEUE_FULL) ? 2 * s->queue_cap : 0;
+            rc = kdop_reserve(s, nc, 0, nq);
+            if (rc != KDOP_OK) break;
+            e = kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
+            r = kdop_get_stats(s, &st);
+          }
+          if (r != KDOP_OK) continue;
+          cudaEventRecord(e0, s->ctx->stream);
+          for (int k = 0; k < repeats; ++k) kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
+          cudaEventRecord(e1, s->ctx->stream);
+          if (cudaEventSynchronize(e1) != cudaSuccess) continue;
+          float ms = 0.f;
+          cudaEventElapsedTime(&ms, e0, e1);
+          if (kdop_get_stats(s, &st) != KDOP_OK) continue;
+          if (ms < best_ms) {
+            best_ms = ms;
+            bo.block_warps = w;
+            bo.stack_cap = c;
+            bo.init_chunk = ch;
+            bo.donate_min = dm;
+          }
+        }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best_ms >= 1e30f) return fail(s->ctx, KDOP_ERR_CUDA, "autotune: no configuration ran");
+  kdop_scene_ext* x = ext(s);
+  x->tuned = bo;
+  x->has_tuned = true;
+  int64_t tets = 0;
+  for (int64_t i = 0; i < n_pairs; ++i) {
+    uint32_t a = x->pairs_host[2 * i], b = x->pairs_host[2 * i + 1];
+    tets += (s->t_off[a + 1] - s->t_off[a]) + (s->t_off[b + 1] - s->t_off[b]);
+  }
+  int size_class = tets > 0 ? (int)std::log2((double)tets) : 0;
+  s->ctx->tuned[std::make_pair(s->K, size_class)] = bo;
+  if (best) *best = bo;
+  return KDOP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,151 @@
+// kdop_internal.h -- host-side structures shared by the C ABI and the kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <limits>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/kdop_cuda.h"
+
+namespace kdop {
+
+constexpr uint32_t LEAF_BIT_HOST = 0x80000000u;
+
+// Unit directions of the K/2 slabs (geometry_direction_table.h:54-176).
+struct DirTable {
+  float d[13][3];
+};
+
+// Device-side control block of one traversal (+ contact generation).
+struct TravCtl {
+  unsigned long long tests;          // node-pair tests
+  unsigned long long leaf_overlaps;  // overlapping leaf pairs before the surface filter
+  unsigned int n_cand;               // candidates emitted (may exceed capacity)
+  unsigned int init_head;            // root pairs claimed
+  unsigned int q_head;               // queue slots claimed by idle warps
+  unsigned int q_tail;               // queue slots reserved by producers
+  int work;                          // outstanding work units; 0 = traversal finished
+  unsigned int error;                // DEV_ERR_* bits
+  unsigned int n_contacts;           // contacts emitted (may exceed capacity)
+  unsigned int n_init;               // root pairs in this launch
+  unsigned int pair_base;            // pair index of the first root pair
+  unsigned int max_stack;            // deepest warp stack seen
+  unsigned int pad[2];
+};
+
+enum : unsigned int {
+  DEV_ERR_TIMEOUT = 1u,
+  DEV_ERR_QUEUE_FULL = 2u,
+  DEV_ERR_BAD_INDEX = 4u,
+};
+
+struct TravParams {
+  int block_warps;
+  int stack_cap;
+  int init_chunk;
+  int donate_min;
+  long long timeout_ns;
+  int surface_filter;
+};
+
+}  // namespace kdop
+
+struct kdop_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 0;
+  size_t smem_optin = 0;
+  std::string err;
+  long long launches = 0;
+  // autotuned traversal options keyed by (K, size class)
+  std::map<std::pair<int, int>, kdop_traverse_opts> tuned;
+};
+
+struct kdop_scene {
+  kdop_ctx* ctx = nullptr;
+  int K = 0;
+  int NW = 0;  // float4 chunks per node record
+  int n_meshes = 0;
+  int64_t nv = 0, nt = 0, nn = 0;
+  int depth = 0;
+  std::vector<int64_t> v_off, t_off, level_off;
+  std::vector<uint32_t> root;  // per mesh root node, 0xFFFFFFFF for an empty mesh
+  kdop::DirTable dirs;
+
+  // device arrays
+  float4* rest = nullptr;
+  float4* world = nullptr;
+  uint4* tets = nullptr;  // global vertex indices
+  uint8_t* surf = nullptr;
+  float4* nodes = nullptr;
+  uint32_t* root_dev = nullptr;
+  float4* quat = nullptr;
+  float4* pos = nullptr;
+  float4* lin_vel = nullptr;
+  float4* ang_vel = nullptr;
+  float* phase_dev = nullptr;  // deformation phase, advanced by the motion kernel
+  float amp = 0.f, w = 0.f, phase = 0.f, phase_rate = 0.f;
+  bool have_world = false;
+
+  // traversal / contacts buffers
+  uint2* pairs = nullptr;
+  int64_t pairs_cap = 0;
+  uint32_t* cand = nullptr;  // 3 * cand_cap: A tets | B tets | pair ids
+  int64_t cand_cap = 0;
+  kdop_contact* contacts = nullptr;
+  int4* records = nullptr;  // per candidate: faces, candidate codes, count, first contact
+  int64_t contact_cap = 0;
+  uint4* q_items = nullptr;
+  uint32_t* q_tags = nullptr;
+  int64_t queue_cap = 0;
+  kdop::TravCtl* ctl = nullptr;
+  kdop::TravCtl* ctl_host = nullptr;  // pinned
+
+  int refit_mode = -1;
+  bool traversed = false;
+  bool contacted = false;
+  int64_t last_pairs = 0;
+  int last_mode = 0;
+  kdop::TravParams last_params{};
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  int64_t device_bytes = 0;
+};
+
+namespace kdop {
+
+// host tree construction (kdop_build.cpp)
+int direction_table(int K, float* out);
+struct ForestBuild {
+  std::vector<int64_t> level_off;          // per level start, size depth+2
+  std::vector<uint32_t> topo;              // 2 per node: start, end (global ids)
+  std::vector<uint32_t> root;              // per mesh
+  int depth = 0;
+};
+// meshes: tet counts and concatenated (global-vertex) tets; t_off per mesh.
+int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t>& n_verts,
+                 const std::vector<const uint32_t*>& tets, const std::vector<int64_t>& n_tets,
+                 const std::vector<int64_t>& t_off, ForestBuild& out);
+void morton_order(const float* xyz, int64_t n_tets, const uint32_t* tets, std::vector<uint32_t>& perm);
+void surface_map(int64_t n_tets, const uint32_t* tets, uint8_t* surf);
+
+// kernel launchers (return cudaGetLastError of the launches)
+cudaError_t launch_write_topology(kdop_scene* s, const uint32_t* topo_dev);
+cudaError_t launch_refit(kdop_scene* s, int mode);
+cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int plain);
+cudaError_t launch_contacts(kdop_scene* s);
+cudaError_t launch_adjoint(kdop_scene* s, const float* dd, const float* dn, float* grad);
+cudaError_t launch_motion(kdop_scene* s);
+cudaError_t launch_world(kdop_scene* s, int mode, float4* out);
+int traverse_block_threads(int block_warps);
+size_t traverse_smem_bytes(int block_warps, int stack_cap);
+cudaError_t traverse_prepare(int K, size_t smem);
+
+}  // namespace kdop

@@ -1,0 +1,296 @@
+// kdop_refit.cu -- bottom-up kDOP refit of every tree of a scene.
+//
+// Reference: kdop::refit_tree (SIMULATION/KDOP/KDOP/include/kdop_refit_tree.h:
+// 24-115 per chunk, 120-162 per tree): a leaf gets make_dop of its tet's four
+// vertices (FOUNDATION/GEOMETRY/GEOMETRY/include/types/geometry_dop.h:49-74),
+// an internal node make_union of its two children (geometry_make_union.h:
+// 10-24).  The OpenCL back-end did one work-group per object with retry loops
+// (cl/kernels/kdop_cl_refit_tree.cl:17-168).
+//
+// Here the forest is stored level by level, so one launch refits one level of
+// every tree at once, deepest level first.  Thread t handles float4 chunk
+// t % NW of node t / NW: consecutive threads write consecutive 16-byte words
+// (fully coalesced stores) and read the same chunk of the two adjacent
+// children.  Leaves transform their vertices on the fly when the scene is in
+// pose or deform mode (narrow_update_kdop_bvh.h:154-165 fused into the leaf
+// pass, so no world-vertex array is written).  The upper levels, too small to
+// fill the GPU, are refitted by one block that walks them with block barriers.
+#include "kdop_device.cuh"
+
+namespace kdop {
+
+template <int K>
+__device__ __forceinline__ float4 refit_chunk(const float4* nodes, int64_t node, int j, const uint4* __restrict__ tets,
+                                              const VertexSource& vs, const DirTable& dt, bool use_ldg) {
+  using L = NodeLayout<K>;
+  float4 tc = use_ldg ? __ldg(nodes + node * L::NW + L::TOPO_CHUNK) : nodes[node * L::NW + L::TOPO_CHUNK];
+  uint32_t start = __float_as_uint(L::TOPO_ZW ? tc.z : tc.x);
+  uint32_t end = __float_as_uint(L::TOPO_ZW ? tc.w : tc.y);
+  float w[4];
+  if (start == end) {
+    uint4 t = __ldg(tets + start);
+    f3 p[4] = {world_vertex(vs, t.x), world_vertex(vs, t.y), world_vertex(vs, t.z), world_vertex(vs, t.w)};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      int s = 2 * j + h;
+      if (s < L::NS) {
+        f3 d = mk3(dt.d[s][0], dt.d[s][1], dt.d[s][2]);
+        float lo = 3.40282346638528859812e+38f, hi = -3.40282346638528859812e+38f;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          float pr = dot3(d, p[v]);
+          lo = smin(lo, pr);
+          hi = smax(hi, pr);
+        }
+        w[2 * h] = lo;
+        w[2 * h + 1] = hi;
+      } else {
+        w[2 * h] = 0.f;
+        w[2 * h + 1] = 0.f;
+      }
+    }
+  } else {
+    float4 a = use_ldg ? __ldg(nodes + (int64_t)start * L::NW + j) : nodes[(int64_t)start * L::NW + j];
+    float4 b = use_ldg ? __ldg(nodes + (int64_t)end * L::NW + j) : nodes[(int64_t)end * L::NW + j];
+    // lo: min(A.lo, B.lo) = (B < A) ? B : A ; hi: max(A.hi, B.hi) = (A < B) ? B : A
+    w[0] = smin(a.x, b.x);
+    w[1] = smax(a.y, b.y);
+    w[2] = smin(a.z, b.z);
+    w[3] = smax(a.w, b.w);
+    if (2 * j + 1 >= L::NS) {
+      w[2] = 0.f;
+      w[3] = 0.f;
+    }
+    if (2 * j >= L::NS) {
+      w[0] = 0.f;
+      w[1] = 0.f;
+    }
+  }
+  if (j == L::TOPO_CHUNK) {
+    if (L::TOPO_ZW) {
+      w[2] = tc.z;
+      w[3] = tc.w;
+    } else {
+      w[0] = tc.x;
+      w[1] = tc.y;
+    }
+  }
+  return make_float4(w[0], w[1], w[2], w[3]);
+}
+
+template <int K>
+__global__ void __launch_bounds__(256) refit_level_kernel(float4* nodes, int64_t begin, int64_t count,
+                                                          const uint4* __restrict__ tets, VertexSource vs,
+                                                          DirTable dt) {
+  using L = NodeLayout<K>;
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count * L::NW) return;
+  int64_t node = begin + t / L::NW;
+  int j = (int)(t % L::NW);
+  float4 o = refit_chunk<K>(nodes, node, j, tets, vs, dt, true);
+  nodes[node * L::NW + j] = o;
+}
+
+// Levels [0, last] of the forest, deepest first, by a single block.
+template <int K>
+__global__ void __launch_bounds__(1024) refit_tail_kernel(float4* nodes, const int64_t* __restrict__ level_off,
+                                                          int last, const uint4* __restrict__ tets,
+                                                          VertexSource vs, DirTable dt) {
+  using L = NodeLayout<K>;
+  for (int d = last; d >= 0; --d) {
+    int64_t b = level_off[d], n = (level_off[d + 1] - b) * L::NW;
+    for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
+      int64_t node = b + t / L::NW;
+      int j = (int)(t % L::NW);
+      float4 o = refit_chunk<K>(nodes, node, j, tets, vs, dt, false);
+      nodes[node * L::NW + j] = o;
+    }
+    __syncthreads();
+  }
+}
+
+// Topology words (start, end) into the node records, slabs zeroed.
+template <int K>
+__global__ void write_topology_kernel(float4* nodes, int64_t nn, const uint32_t* __restrict__ topo) {
+  using L = NodeLayout<K>;
+  int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nn * L::NW) return;
+  int64_t node = t / L::NW;
+  int j = (int)(t % L::NW);
+  float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (j == L::TOPO_CHUNK) {
+    float a = __uint_as_float(topo[2 * node]), b = __uint_as_float(topo[2 * node + 1]);
+    if (L::TOPO_ZW) {
+      o.z = a;
+      o.w = b;
+    } else {
+      o.x = a;
+      o.y = b;
+    }
+  }
+  nodes[t] = o;
+}
+
+// World positions of all vertices (pose / deform modes), for read-back.
+__global__ void world_kernel(int64_t nv, VertexSource vs, float4* out) {
+  int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  f3 x = world_vertex(vs, (uint32_t)v);
+  out[v] = make_float4(x.x, x.y, x.z, 0.f);
+}
+
+// One step of rigid motion per mesh and of the deformation phase:
+// p += v, q = normalise(q + 0.5 (0, w) q).
+__global__ void motion_kernel(int n_meshes, float4* quat, float4* pos, const float4* __restrict__ lin,
+                              const float4* __restrict__ ang, float* phase, float phase_rate) {
+  int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m == 0) *phase = *phase + phase_rate;
+  if (m >= n_meshes) return;
+  float4 p = pos[m], v = lin[m], q = quat[m], w = ang[m];
+  p.x += v.x;
+  p.y += v.y;
+  p.z += v.z;
+  // dq = 0.5 * (0, w) (x) q
+  float dw = -(w.x * q.y + w.y * q.z + w.z * q.w);
+  float dx = w.x * q.x + (w.y * q.w - w.z * q.z);
+  float dy = w.y * q.x + (w.z * q.y - w.x * q.w);
+  float dz = w.z * q.x + (w.x * q.z - w.y * q.y);
+  q.x += 0.5f * dw;
+  q.y += 0.5f * dx;
+  q.z += 0.5f * dy;
+  q.w += 0.5f * dz;
+  float inv = rsqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+  q.x *= inv;
+  q.y *= inv;
+  q.z *= inv;
+  q.w *= inv;
+  quat[m] = q;
+  pos[m] = p;
+}
+
+// xyz triples -> float4 (w = mesh index bits when with_mesh_id >= 0, else 0)
+__global__ void pack3_kernel(const float* __restrict__ in, float4* out, int64_t n, const float4* __restrict__ keep_w,
+                             int keep) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float w = keep ? keep_w[i].w : 0.f;
+  out[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], w);
+}
+__global__ void pack4_kernel(const float* __restrict__ in, float4* out, int64_t n) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = make_float4(in[4 * i], in[4 * i + 1], in[4 * i + 2], in[4 * i + 3]);
+}
+
+cudaError_t launch_pack3(kdop_scene* s, const float* in, float4* out, int64_t n, int with_mesh_id) {
+  if (n <= 0) return cudaSuccess;
+  pack3_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->ctx->stream>>>(in, out, n, s->rest, with_mesh_id >= 0);
+  s->ctx->launches++;
+  return cudaGetLastError();
+}
+cudaError_t launch_pack4(kdop_scene* s, const float* in, float4* out, int64_t n) {
+  if (n <= 0) return cudaSuccess;
+  pack4_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s->ctx->stream>>>(in, out, n);
+  s->ctx->launches++;
+  return cudaGetLastError();
+}
+
+static VertexSource vertex_source(kdop_scene* s, int mode) {
+  VertexSource vs;
+  vs.rest = s->rest;
+  vs.world = s->world;
+  vs.quat = s->quat;
+  vs.pos = s->pos;
+  vs.deform.amp = s->amp;
+  vs.deform.w = s->w;
+  vs.deform.phase = s->phase_dev;
+  vs.mode = mode;
+  return vs;
+}
+
+// Device copy of the level offsets for the tail kernel (lives in the scene's
+// root_dev allocation after the per-mesh roots).
+static const int64_t* level_off_dev(kdop_scene* s) {
+  return reinterpret_cast<const int64_t*>(s->root_dev + ((s->n_meshes + 1) & ~1));
+}
+
+template <int K>
+static cudaError_t refit_impl(kdop_scene* s, int mode) {
+  using L = NodeLayout<K>;
+  VertexSource vs = vertex_source(s, mode);
+  const int64_t small = 16384;
+  int levels = (int)s->level_off.size() - 1;
+  if (levels <= 0) return cudaSuccess;
+  int tail = -1;  // levels [0, tail] go to the single-block kernel
+  for (int d = 0; d < levels; ++d) {
+    if ((s->level_off[d + 1] - s->level_off[d]) * L::NW <= small)
+      tail = d;
+    else
+      break;
+  }
+  for (int d = levels - 1; d > tail; --d) {
+    int64_t b = s->level_off[d], n = s->level_off[d + 1] - b;
+    int64_t items = n * L::NW;
+    unsigned grid = (unsigned)((items + 255) / 256);
+    refit_level_kernel<K><<<grid, 256, 0, s->ctx->stream>>>(s->nodes, b, n, s->tets, vs, s->dirs);
+    s->ctx->launches++;
+  }
+  if (tail >= 0) {
+    refit_tail_kernel<K><<<1, 1024, 0, s->ctx->stream>>>(s->nodes, level_off_dev(s), tail, s->tets, vs, s->dirs);
+    s->ctx->launches++;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refit(kdop_scene* s, int mode) {
+  switch (s->K) {
+    case 6: return refit_impl<6>(s, mode);
+    case 8: return refit_impl<8>(s, mode);
+    case 12: return refit_impl<12>(s, mode);
+    case 14: return refit_impl<14>(s, mode);
+    case 18: return refit_impl<18>(s, mode);
+    case 20: return refit_impl<20>(s, mode);
+    case 26: return refit_impl<26>(s, mode);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <int K>
+static cudaError_t topo_impl(kdop_scene* s, const uint32_t* topo) {
+  int64_t items = s->nn * NodeLayout<K>::NW;
+  if (items == 0) return cudaSuccess;
+  write_topology_kernel<K><<<(unsigned)((items + 255) / 256), 256, 0, s->ctx->stream>>>(s->nodes, s->nn, topo);
+  s->ctx->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_write_topology(kdop_scene* s, const uint32_t* topo) {
+  switch (s->K) {
+    case 6: return topo_impl<6>(s, topo);
+    case 8: return topo_impl<8>(s, topo);
+    case 12: return topo_impl<12>(s, topo);
+    case 14: return topo_impl<14>(s, topo);
+    case 18: return topo_impl<18>(s, topo);
+    case 20: return topo_impl<20>(s, topo);
+    case 26: return topo_impl<26>(s, topo);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_world(kdop_scene* s, int mode, float4* out) {
+  if (s->nv == 0) return cudaSuccess;
+  VertexSource vs = vertex_source(s, mode);
+  world_kernel<<<(unsigned)((s->nv + 255) / 256), 256, 0, s->ctx->stream>>>(s->nv, vs, out);
+  s->ctx->launches++;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_motion(kdop_scene* s) {
+  int n = s->n_meshes > 0 ? s->n_meshes : 1;
+  motion_kernel<<<(n + 127) / 128, 128, 0, s->ctx->stream>>>(s->n_meshes, s->quat, s->pos, s->lin_vel, s->ang_vel,
+                                                              s->phase_dev, s->phase_rate);
+  s->ctx->launches++;
+  return cudaGetLastError();
+}
+
+}  // namespace kdop

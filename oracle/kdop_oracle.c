@@ -237,10 +237,10 @@ int or_traverse_f(int K, const float* volA, const int64_t* leftA, const int64_t*
   return t.over ? -1 : 0;
 }
 
-int or_run_pair_f(int K, int64_t nvA, const float* xyzA, int64_t ntA, const uint32_t* tetsA,
-                  const uint8_t* surfA, int64_t nvB, const float* xyzB, int64_t ntB, const uint32_t* tetsB,
-                  const uint8_t* surfB, int64_t cap, uint32_t* out_pairs, int64_t* npairs, int64_t* tests,
-                  int64_t* leaf_overlaps) {
+int or_run_pair_f(int K, int64_t nvA, const float* xyzA, const float* restA, int64_t ntA, const uint32_t* tetsA,
+                  const uint8_t* surfA, int64_t nvB, const float* xyzB, const float* restB, int64_t ntB,
+                  const uint32_t* tetsB, const uint8_t* surfB, int64_t cap, uint32_t* out_pairs, int64_t* npairs,
+                  int64_t* tests, int64_t* leaf_overlaps) {
   *npairs = *tests = *leaf_overlaps = 0;
   if (ntA <= 0 || ntB <= 0) return 0;
   int64_t nnA = 2 * ntA - 1, nnB = 2 * ntB - 1;
@@ -252,8 +252,8 @@ int or_run_pair_f(int K, int64_t nvA, const float* xyzA, int64_t ntA, const uint
   float* vB = (float*)malloc(4 * (size_t)K * (size_t)nnB);
   int rc = -2;
   if (pA && pB && tA && tB && vA && vB) {
-    or_morton_order(xyzA, nvA, ntA, tetsA, pA);
-    or_morton_order(xyzB, nvB, ntB, tetsB, pB);
+    or_morton_order(restA ? restA : xyzA, nvA, ntA, tetsA, pA);
+    or_morton_order(restB ? restB : xyzB, nvB, ntB, tetsB, pB);
     or_build_tree(ntA, pA, tA, tA + nnA, tA + 2 * nnA);
     or_build_tree(ntB, pB, tB, tB + nnB, tB + 2 * nnB);
     or_refit_f(K, xyzA, tetsA, nnA, tA, tA + nnA, tA + 2 * nnA, vA);
@@ -270,6 +270,7 @@ typedef struct {
   int K;
   const int64_t *v_off, *t_off;
   const float* xyz;
+  const float* rest;
   const uint32_t* tets;
   const uint8_t* surf;
   const uint32_t* pairs;
@@ -294,10 +295,11 @@ static void* or_pool_worker(void* arg) {
     for (;;) {
       uint32_t* buf = (uint32_t*)malloc(8 * (size_t)cap);
       int64_t np = 0, tests = 0, lo = 0;
-      int rc = or_run_pair_f(P->K, P->v_off[a + 1] - P->v_off[a], P->xyz + 3 * P->v_off[a], ntA,
-                             P->tets + 4 * P->t_off[a], P->surf + P->t_off[a], P->v_off[b + 1] - P->v_off[b],
-                             P->xyz + 3 * P->v_off[b], ntB, P->tets + 4 * P->t_off[b], P->surf + P->t_off[b], cap,
-                             buf, &np, &tests, &lo);
+      int rc = or_run_pair_f(P->K, P->v_off[a + 1] - P->v_off[a], P->xyz + 3 * P->v_off[a],
+                             P->rest ? P->rest + 3 * P->v_off[a] : NULL, ntA, P->tets + 4 * P->t_off[a],
+                             P->surf + P->t_off[a], P->v_off[b + 1] - P->v_off[b], P->xyz + 3 * P->v_off[b],
+                             P->rest ? P->rest + 3 * P->v_off[b] : NULL, ntB, P->tets + 4 * P->t_off[b],
+                             P->surf + P->t_off[b], cap, buf, &np, &tests, &lo);
       if (rc == -1) {
         free(buf);
         cap = np + 16;
@@ -313,14 +315,14 @@ static void* or_pool_worker(void* arg) {
   return NULL;
 }
 
-int or_run_pairs_f(int K, int n_meshes, const int64_t* v_off, const float* xyz, const int64_t* t_off,
+int or_run_pairs_f(int K, int n_meshes, const int64_t* v_off, const float* xyz, const float* rest, const int64_t* t_off,
                    const uint32_t* tets, const uint8_t* surf, int64_t n_pairs, const uint32_t* pairs,
                    int threads, int64_t cap, uint32_t* out_pairs, int64_t* npairs, int64_t* tests_per_pair,
                    int64_t* pairs_per_pair) {
   (void)n_meshes;
   or_pool P;
   memset(&P, 0, sizeof(P));
-  P.K = K; P.v_off = v_off; P.t_off = t_off; P.xyz = xyz; P.tets = tets; P.surf = surf;
+  P.K = K; P.v_off = v_off; P.t_off = t_off; P.xyz = xyz; P.rest = rest; P.tets = tets; P.surf = surf;
   P.pairs = pairs; P.n_pairs = n_pairs;
   pthread_mutex_init(&P.mu, NULL);
   P.res = (uint32_t**)calloc((size_t)(n_pairs > 0 ? n_pairs : 1), sizeof(uint32_t*));

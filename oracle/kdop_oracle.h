@@ -67,16 +67,19 @@ int or_traverse_f(int K, const float* volA, const int64_t* leftA, const int64_t*
                   const int64_t* tetB, const uint8_t* surfB, int64_t cap, uint32_t* out_pairs,
                   int64_t* npairs, int64_t* tests, int64_t* leaf_overlaps);
 
-/* One mesh pair end to end: Morton order, tree build, refit, traversal. */
-int or_run_pair_f(int K, int64_t nvA, const float* xyzA, int64_t ntA, const uint32_t* tetsA,
-                  const uint8_t* surfA, int64_t nvB, const float* xyzB, int64_t ntB, const uint32_t* tetsB,
-                  const uint8_t* surfB, int64_t cap, uint32_t* out_pairs, int64_t* npairs, int64_t* tests,
-                  int64_t* leaf_overlaps);
+/* One mesh pair end to end: Morton order and tree build on the rest
+ * positions restA/restB (NULL: the world positions), refit on the world
+ * positions xyzA/xyzB, traversal. */
+int or_run_pair_f(int K, int64_t nvA, const float* xyzA, const float* restA, int64_t ntA, const uint32_t* tetsA,
+                  const uint8_t* surfA, int64_t nvB, const float* xyzB, const float* restB, int64_t ntB,
+                  const uint32_t* tetsB, const uint8_t* surfB, int64_t cap, uint32_t* out_pairs, int64_t* npairs,
+                  int64_t* tests, int64_t* leaf_overlaps);
 
 /* Many independent mesh pairs with a thread pool (threads <= 0: all cores).
  * Meshes are concatenated: vertices xyz[v_off[m]..v_off[m+1]), tets likewise
- * with mesh-local vertex indices.  out_pairs rows are (pair, a, b). */
-int or_run_pairs_f(int K, int n_meshes, const int64_t* v_off, const float* xyz, const int64_t* t_off,
+ * with mesh-local vertex indices; rest (or NULL) gives the tree-building
+ * positions.  out_pairs rows are (pair, a, b). */
+int or_run_pairs_f(int K, int n_meshes, const int64_t* v_off, const float* xyz, const float* rest, const int64_t* t_off,
                    const uint32_t* tets, const uint8_t* surf, int64_t n_pairs, const uint32_t* pairs,
                    int threads, int64_t cap, uint32_t* out_pairs, int64_t* npairs, int64_t* tests_per_pair,
                    int64_t* pairs_per_pair);

@@ -61,8 +61,10 @@ class Oracle:
         L.or_build_tree.argtypes = [_i64, _p, _p, _p, _p]
         L.or_build_tree.restype = _i64
         L.or_refit_f.argtypes = [C.c_int, _p, _p, _i64, _p, _p, _p, _p]
-        L.or_run_pair_f.argtypes = [C.c_int, _i64, _p, _i64, _p, _p, _i64, _p, _i64, _p, _p, _i64, _p, _p, _p, _p]
-        L.or_run_pairs_f.argtypes = [C.c_int, C.c_int, _p, _p, _p, _p, _p, _i64, _p, C.c_int, _i64, _p, _p, _p, _p]
+        L.or_run_pair_f.argtypes = [C.c_int, _i64, _p, _p, _i64, _p, _p, _i64, _p, _p, _i64, _p, _p, _i64, _p, _p,
+                                    _p, _p]
+        L.or_run_pairs_f.argtypes = [C.c_int, C.c_int, _p, _p, _p, _p, _p, _p, _i64, _p, C.c_int, _i64, _p, _p, _p,
+                                     _p]
         L.or_surface_map.argtypes = [_i64, _i64, _p, _p]
         for nm in ("or_contacts_f", "or_contacts_d", "or_contacts_dd"):
             getattr(L, nm).argtypes = [_p, _p, _p, _p, _p, _p, _i64, _p, _i64, _p, _p, _p]
@@ -111,17 +113,21 @@ class Oracle:
                             _ptr(_c(right, np.int64)), _ptr(_c(tet, np.int64)), _ptr(vol))
         return vol
 
-    def run_pair(self, K, xyzA, tetsA, surfA, xyzB, tetsB, surfB):
-        """Sorted-by-traversal-order pairs (n,2), node-pair tests, leaf overlaps."""
+    def run_pair(self, K, xyzA, tetsA, surfA, xyzB, tetsB, surfB, restA=None, restB=None):
+        """Pairs (n,2) in traversal order, node-pair tests, leaf overlaps.
+        Trees are built on restA/restB (default: the world positions)."""
         xyzA, tetsA, surfA = _c(xyzA, np.float32), _c(tetsA, np.uint32), _c(surfA, np.uint8)
         xyzB, tetsB, surfB = _c(xyzB, np.float32), _c(tetsB, np.uint32), _c(surfB, np.uint8)
+        restA = None if restA is None else _c(restA, np.float32)
+        restB = None if restB is None else _c(restB, np.float32)
         cap = 1 << 16
         while True:
             out = np.zeros((cap, 2), np.uint32)
             np_, tests, lo = _i64(), _i64(), _i64()
-            rc = self.lib.or_run_pair_f(K, xyzA.shape[0], _ptr(xyzA), tetsA.shape[0], _ptr(tetsA), _ptr(surfA),
-                                        xyzB.shape[0], _ptr(xyzB), tetsB.shape[0], _ptr(tetsB), _ptr(surfB), cap,
-                                        _ptr(out), C.byref(np_), C.byref(tests), C.byref(lo))
+            rc = self.lib.or_run_pair_f(K, xyzA.shape[0], _ptr(xyzA), _ptr(restA), tetsA.shape[0], _ptr(tetsA),
+                                        _ptr(surfA), xyzB.shape[0], _ptr(xyzB), _ptr(restB), tetsB.shape[0],
+                                        _ptr(tetsB), _ptr(surfB), cap, _ptr(out), C.byref(np_), C.byref(tests),
+                                        C.byref(lo))
             if rc == -1:
                 cap = np_.value + 16
                 continue
@@ -129,9 +135,11 @@ class Oracle:
                 raise RuntimeError(f"or_run_pair_f failed: {rc}")
             return out[:np_.value].copy(), tests.value, lo.value
 
-    def run_pairs(self, K, meshes_xyz_world, meshes, pairs, threads=0):
-        """Many pairs; meshes_xyz_world[i] are mesh i's world vertices.
-        Returns (rows (n,3) = pair, a, b; tests per pair; pairs per pair)."""
+    def run_pairs(self, K, meshes_xyz_world, meshes, pairs, threads=0, rest=True):
+        """Many pairs; meshes_xyz_world[i] are mesh i's world vertices, trees
+        are built on the meshes' rest positions (rest=True) or on the world
+        positions.  Returns (rows (n,3) = pair, a, b; tests per pair; pairs
+        per pair)."""
         n = len(meshes)
         v_off = np.zeros(n + 1, np.int64)
         t_off = np.zeros(n + 1, np.int64)
@@ -139,6 +147,7 @@ class Oracle:
             v_off[i + 1] = v_off[i] + m.n_verts
             t_off[i + 1] = t_off[i] + m.n_tets
         xyz = _c(np.concatenate(meshes_xyz_world, axis=0), np.float32)
+        rxyz = _c(np.concatenate([m.xyz for m in meshes], axis=0), np.float32) if rest else None
         tets = _c(np.concatenate([m.tets for m in meshes], axis=0), np.uint32)
         surf = _c(np.concatenate([m.surf for m in meshes], axis=0), np.uint8)
         pairs = _c(pairs, np.uint32)
@@ -149,7 +158,8 @@ class Oracle:
         while True:
             out = np.zeros((cap, 3), np.uint32)
             nout = _i64()
-            rc = self.lib.or_run_pairs_f(K, n, _ptr(v_off), _ptr(xyz), _ptr(t_off), _ptr(tets), _ptr(surf), npairs,
+            rc = self.lib.or_run_pairs_f(K, n, _ptr(v_off), _ptr(xyz), _ptr(rxyz), _ptr(t_off), _ptr(tets), _ptr(surf),
+                                         npairs,
                                          _ptr(pairs), threads, cap, _ptr(out), C.byref(nout), _ptr(tpp), _ptr(ppp))
             if rc == -1:
                 cap = nout.value + 16
@@ -231,11 +241,9 @@ class Reference:
         L.ref_direction_table.argtypes = [C.c_int, _p]
         L.ref_contacts_pairs.argtypes = [C.c_int, _p, _p, _p, _p, _p, _p, C.c_longlong, _p, C.c_longlong, _p, _p]
         if hasattr(L, "ref_traverse"):
-            L.ref_traverse.argtypes = [C.c_int, C.c_ulonglong, C.c_int, C.c_int, _p, C.c_int, _p, C.c_int, _p,
-                                       C.c_int, _p, C.c_longlong, _p, _p, C.c_longlong, _p, _p, _p, C.c_longlong,
-                                       _p, _p, _p]
-        L.ref_time_pairs.argtypes = [C.c_int, C.c_ulonglong, C.c_int, _p, _p, _p, _p, C.c_longlong, _p, C.c_int,
-                                     _p, _p]
+            L.ref_traverse.argtypes = [C.c_int, C.c_ulonglong, C.c_int, C.c_int, _p, _p, _p, C.c_int, _p,
+                                       C.c_int, _p, _p, _p, C.c_int, _p, C.c_longlong, _p, _p, C.c_longlong, _p,
+                                       _p, _p, C.c_longlong, _p, _p, _p]
 
     def surface_map(self, xyz, tets) -> np.ndarray:
         xyz, tets = _c(xyz, np.float32), _c(tets, np.uint32)
@@ -281,13 +289,16 @@ class Reference:
                 continue
             return out[:n.value].copy()
 
-    def traverse(self, K, xyzA, tetsA, xyzB, tetsB, mem_bytes=(1 << 64) - 1, reorder=True, want_volumes=False):
-        """Reference refit + tandem traversal of one pair.  Returns dict with
+    def traverse(self, K, restA, qA, pA, tetsA, restB, qB, pB, tetsB, mem_bytes=(1 << 64) - 1, reorder=True,
+                 want_volumes=False):
+        """One pair through the reference pipeline: reorder + tree on the rest
+        positions, pose (q, p), refit, tandem traversal.  Returns dict with
         pairs (n,2) in the caller's tet numbering (traversal order), contacts
         (m,8) rows p3 n3 d pair-row, tests, and optionally the preorder node
         volumes / leaf tets of tree A (one-chunk trees only)."""
-        xyzA, tetsA = _c(xyzA, np.float32), _c(tetsA, np.uint32)
-        xyzB, tetsB = _c(xyzB, np.float32), _c(tetsB, np.uint32)
+        xyzA, tetsA = _c(restA, np.float32), _c(tetsA, np.uint32)
+        xyzB, tetsB = _c(restB, np.float32), _c(tetsB, np.uint32)
+        qA, pA, qB, pB = _c(qA, np.float32), _c(pA, np.float32), _c(qB, np.float32), _c(pB, np.float32)
         capp, capc = 1 << 16, 1 << 17
         nn = 2 * tetsA.shape[0] - 1
         while True:
@@ -297,8 +308,9 @@ class Reference:
             leaf = np.zeros(nn, np.int64) if want_volumes else None
             npairs, ncont, tests, nnodes = C.c_longlong(), C.c_longlong(), C.c_longlong(), C.c_longlong()
             rc = self.lib.ref_traverse(K, C.c_ulonglong(mem_bytes), 1 if reorder else 0, xyzA.shape[0], _ptr(xyzA),
-                                       tetsA.shape[0], _ptr(tetsA), xyzB.shape[0], _ptr(xyzB), tetsB.shape[0],
-                                       _ptr(tetsB), capp, _ptr(pairs), C.byref(npairs), capc, _ptr(cont),
+                                       _ptr(qA), _ptr(pA), tetsA.shape[0], _ptr(tetsA), xyzB.shape[0], _ptr(xyzB),
+                                       _ptr(qB), _ptr(pB), tetsB.shape[0], _ptr(tetsB), capp, _ptr(pairs),
+                                       C.byref(npairs), capc, _ptr(cont),
                                        C.byref(ncont), C.byref(tests), nn if want_volumes else 0, _ptr(vols),
                                        _ptr(leaf), C.byref(nnodes))
             if rc != 0:
@@ -319,23 +331,28 @@ class RefTimer:
 
     def __init__(self, path: str = REF_TIME_SO):
         self.lib = C.CDLL(path)
-        self.lib.ref_time_pairs.argtypes = [C.c_int, C.c_ulonglong, C.c_int, _p, _p, _p, _p, C.c_longlong, _p,
-                                            C.c_int, _p, _p]
+        self.lib.ref_time_pairs.argtypes = [C.c_int, C.c_ulonglong, C.c_int, _p, _p, _p, _p, _p, _p, C.c_longlong,
+                                            _p, C.c_int, _p, _p]
 
-    def time_pairs(self, K, meshes_world_xyz, meshes, pairs, threads=1, mem_bytes=(1 << 64) - 1):
+    def time_pairs(self, K, meshes, quat, pos, pairs, threads=1, mem_bytes=(1 << 64) - 1):
+        """Seconds for one simulation step of the reference over `pairs`:
+        per pair, pose + refit of both meshes and the tandem traversal with
+        contact generation (trees set up untimed on the rest positions)."""
         n = len(meshes)
         v_off = np.zeros(n + 1, np.int64)
         t_off = np.zeros(n + 1, np.int64)
         for i, m in enumerate(meshes):
             v_off[i + 1] = v_off[i] + m.n_verts
             t_off[i + 1] = t_off[i] + m.n_tets
-        xyz = _c(np.concatenate(meshes_world_xyz, axis=0), np.float32)
+        xyz = _c(np.concatenate([m.xyz for m in meshes], axis=0), np.float32)
         tets = _c(np.concatenate([m.tets for m in meshes], axis=0), np.uint32)
+        quat, pos = _c(quat, np.float32), _c(pos, np.float32)
         pairs = _c(pairs, np.uint32)
         sec = C.c_double()
         cont = C.c_longlong()
-        rc = self.lib.ref_time_pairs(K, C.c_ulonglong(mem_bytes), n, _ptr(v_off), _ptr(xyz), _ptr(t_off), _ptr(tets),
-                                     pairs.shape[0], _ptr(pairs), threads, C.byref(sec), C.byref(cont))
+        rc = self.lib.ref_time_pairs(K, C.c_ulonglong(mem_bytes), n, _ptr(v_off), _ptr(xyz), _ptr(quat), _ptr(pos),
+                                     _ptr(t_off), _ptr(tets), pairs.shape[0], _ptr(pairs), threads, C.byref(sec),
+                                     C.byref(cont))
         if rc != 0:
             raise RuntimeError(f"ref_time_pairs failed: {rc}")
         return sec.value, cont.value

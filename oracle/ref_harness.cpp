@@ -15,7 +15,14 @@
 //                 and record every leaf pair that reaches contact generation
 //                 (kdop_tandem_traversal.h:116).
 //   REF_RECORD=0  libkdop_ref_time.so: the unmodified reference headers, used
-//                 to time the reference's refit + tandem traversal.
+//                 to time the reference's per-step hot path.
+//
+// Both follow the reference's pipeline: scene set-up reorders each mesh
+// (Morton, narrow_shape_types.h:172), computes its surface map (:182) and
+// builds its tree on the rest positions (narrow_object.h:121); each step
+// poses the vertices and refits (narrow_update_kdop_bvh.h:146-171), then runs
+// the tandem traversal with contact generation
+// (narrow_tetramesh_tetramesh.h:68-85 -> kdop_tandem_traversal.h:199-226).
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -104,6 +111,7 @@ struct Mesh {
   T4Mesh mesh;
   mesh_array::VertexAttribute<T, T4Mesh> X, Y, Z;
   mesh_array::TetrahedronAttribute<mesh_array::TetrahedronSurfaceInfo, T4Mesh> surf;
+  std::vector<T> rest;  // rest positions in this mesh's vertex order
 };
 
 template <typename T>
@@ -122,6 +130,39 @@ static void make_mesh(Mesh<T>& m, int nv, float const* xyz, int nt, unsigned con
     m.X(v) = (T)xyz[3 * i + 0];
     m.Y(v) = (T)xyz[3 * i + 1];
     m.Z(v) = (T)xyz[3 * i + 2];
+  }
+}
+
+// Copy the current X, Y, Z as the rest positions.
+template <typename T>
+static void keep_rest(Mesh<T>& m) {
+  size_t N = m.mesh.vertex_size();
+  m.rest.resize(3 * N);
+  for (size_t n = 0; n < N; ++n) {
+    mesh_array::Vertex const& v = m.mesh.vertex(n);
+    m.rest[3 * n] = m.X(v);
+    m.rest[3 * n + 1] = m.Y(v);
+    m.rest[3 * n + 2] = m.Z(v);
+  }
+}
+
+// The rigid transform of narrow::update_kdop_bvh
+// (SIMULATION/NARROW/NARROW/include/narrow_update_kdop_bvh.h:154-165):
+// X = tiny::rotate(q, rest) + p for every vertex, q = (w, x, y, z).
+template <typename T>
+static void pose_mesh(Mesh<T>& m, float const* q, float const* p) {
+  typedef tiny::MathTypes<T> M;
+  typedef typename M::vector3_type V;
+  typename M::quaternion_type Q((T)q[0], (T)q[1], (T)q[2], (T)q[3]);
+  V P = V::make((T)p[0], (T)p[1], (T)p[2]);
+  size_t N = m.mesh.vertex_size();
+  for (size_t n = 0; n < N; ++n) {
+    mesh_array::Vertex const& v = m.mesh.vertex(n);
+    V r0 = V::make(m.rest[3 * n], m.rest[3 * n + 1], m.rest[3 * n + 2]);
+    V r = tiny::rotate(Q, r0) + P;
+    m.X(v) = r(0);
+    m.Y(v) = r(1);
+    m.Z(v) = r(2);
   }
 }
 
@@ -146,10 +187,17 @@ static Key key_of(T const* c12) {
   }
   return k;
 }
-static Key key_of_tet(float const* xyz, unsigned const* tet) {
+template <typename T>
+static Key key_of_mesh_tet(Mesh<T> const& m, size_t t) {
+  mesh_array::Tetrahedron const& tet = m.mesh.tetrahedron(t);
+  size_t vi[4] = {tet.i(), tet.j(), tet.k(), tet.m()};
   float c[12];
-  for (int v = 0; v < 4; ++v)
-    for (int d = 0; d < 3; ++d) c[3 * v + d] = xyz[3 * tet[v] + d];
+  for (int v = 0; v < 4; ++v) {
+    mesh_array::Vertex const& vv = m.mesh.vertex(vi[v]);
+    c[3 * v + 0] = (float)m.X(vv);
+    c[3 * v + 1] = (float)m.Y(vv);
+    c[3 * v + 2] = (float)m.Z(vv);
+  }
   return key_of(c);
 }
 
@@ -223,35 +271,55 @@ static void walk(kdop::SubTree<T, K> const& st, size_t idx, std::vector<float>& 
   walk<T, K>(st, n.m_end, vols, leaf);
 }
 
+// Scene set-up of one mesh: reorder (optional), surface map, tree on rest.
+template <typename T, size_t K>
+static void setup_mesh(int nv, float const* rest, int nt, unsigned const* tets, int reorder,
+                       unsigned long long mem_bytes, Mesh<T>& out, kdop::Tree<T, K>& tree) {
+  typedef typename tiny::MathTypes<T>::vector3_type V;
+  if (reorder) {
+    Mesh<T> raw;
+    make_mesh(raw, nv, rest, nt, tets);
+    reorder_mesh(raw, out);
+  } else {
+    make_mesh(out, nv, rest, nt, tets);
+  }
+  mesh_array::compute_surface_map(out.mesh, out.X, out.Y, out.Z, out.surf);
+  keep_rest(out);
+  tree = kdop::make_tree<V, K, T>((size_t)mem_bytes, out.mesh, out.X, out.Y, out.Z, kdop::sequential());
+}
+
 #if REF_RECORD
+// One mesh pair through set-up and one simulation step, recording the leaf
+// pairs (in the caller's tet numbering), the contacts and the test count.
 template <size_t K>
-static int traverse_k(unsigned long long mem_bytes, int reorder, int nvA, float const* xyzA, int ntA,
-                      unsigned const* tetsA, int nvB, float const* xyzB, int ntB, unsigned const* tetsB,
-                      long long cap_pairs, unsigned* out_pairs, long long* out_npairs,
-                      long long cap_contacts, float* out_contacts, long long* out_ncontacts,
+static int traverse_k(unsigned long long mem_bytes, int reorder, int nvA, float const* restA, float const* qA,
+                      float const* pA, int ntA, unsigned const* tetsA, int nvB, float const* restB, float const* qB,
+                      float const* pB, int ntB, unsigned const* tetsB, long long cap_pairs, unsigned* out_pairs,
+                      long long* out_npairs, long long cap_contacts, float* out_contacts, long long* out_ncontacts,
                       long long* out_tests, long long cap_nodes, float* out_volsA, long long* out_leafA,
                       long long* out_nnodesA) {
   typedef float T;
   typedef tiny::MathTypes<T>::vector3_type V;
-  Mesh<T> a0, b0, a, b;
-  make_mesh(a0, nvA, xyzA, ntA, tetsA);
-  make_mesh(b0, nvB, xyzB, ntB, tetsB);
-  Mesh<T>* pa = &a0;
-  Mesh<T>* pb = &b0;
-  if (reorder) {
-    reorder_mesh(a0, a);
-    reorder_mesh(b0, b);
-    pa = &a;
-    pb = &b;
-  }
-  mesh_array::compute_surface_map(pa->mesh, pa->X, pa->Y, pa->Z, pa->surf);
-  mesh_array::compute_surface_map(pb->mesh, pb->X, pb->Y, pb->Z, pb->surf);
-  std::map<Key, unsigned> mapA, mapB;
-  for (int t = 0; t < ntA; ++t) mapA[key_of_tet(xyzA, tetsA + 4 * t)] = (unsigned)t;
-  for (int t = 0; t < ntB; ++t) mapB[key_of_tet(xyzB, tetsB + 4 * t)] = (unsigned)t;
+  Mesh<T> a, b;
+  kdop::Tree<T, K> ta, tb;
+  setup_mesh<T, K>(nvA, restA, ntA, tetsA, reorder, mem_bytes, a, ta);
+  setup_mesh<T, K>(nvB, restB, ntB, tetsB, reorder, mem_bytes, b, tb);
+  pose_mesh(a, qA, pA);
+  kdop::refit_tree<V, K, T>(ta, a.mesh, a.X, a.Y, a.Z, kdop::sequential());
+  pose_mesh(b, qB, pB);
+  kdop::refit_tree<V, K, T>(tb, b.mesh, b.X, b.Y, b.Z, kdop::sequential());
 
-  kdop::Tree<T, K> ta = kdop::make_tree<V, K, T>((size_t)mem_bytes, pa->mesh, pa->X, pa->Y, pa->Z, kdop::sequential());
-  kdop::Tree<T, K> tb = kdop::make_tree<V, K, T>((size_t)mem_bytes, pb->mesh, pb->X, pb->Y, pb->Z, kdop::sequential());
+  // caller's tet numbering, keyed by the posed coordinates of the input meshes
+  Mesh<T> a0, b0;
+  make_mesh(a0, nvA, restA, ntA, tetsA);
+  make_mesh(b0, nvB, restB, ntB, tetsB);
+  keep_rest(a0);
+  keep_rest(b0);
+  pose_mesh(a0, qA, pA);
+  pose_mesh(b0, qB, pB);
+  std::map<Key, unsigned> mapA, mapB;
+  for (int t = 0; t < ntA; ++t) mapA[key_of_mesh_tet(a0, (size_t)t)] = (unsigned)t;
+  for (int t = 0; t < ntB; ++t) mapB[key_of_mesh_tet(b0, (size_t)t)] = (unsigned)t;
 
   if (out_volsA && ta.number_of_levels() == 1 && ta.branches().size() == 1) {
     std::vector<float> vols;
@@ -263,17 +331,7 @@ static int traverse_k(unsigned long long mem_bytes, int reorder, int nvA, float 
       for (size_t i = 0; i < leaf.size(); ++i) {
         long long t = leaf[i];
         if (t >= 0) {
-          // map reordered tet id back to the caller's numbering
-          mesh_array::Tetrahedron const& tet = pa->mesh.tetrahedron((size_t)t);
-          float c[12];
-          size_t vi[4] = {tet.i(), tet.j(), tet.k(), tet.m()};
-          for (int v = 0; v < 4; ++v) {
-            mesh_array::Vertex const& vv = pa->mesh.vertex(vi[v]);
-            c[3 * v + 0] = pa->X(vv);
-            c[3 * v + 1] = pa->Y(vv);
-            c[3 * v + 2] = pa->Z(vv);
-          }
-          std::map<Key, unsigned>::const_iterator it = mapA.find(key_of(c));
+          std::map<Key, unsigned>::const_iterator it = mapA.find(key_of_mesh_tet(a, (size_t)t));
           t = (it == mapA.end()) ? -2 : (long long)it->second;
         }
         out_leafA[i] = t;
@@ -287,8 +345,7 @@ static int traverse_k(unsigned long long mem_bytes, int reorder, int nvA, float 
   rec.mapB = &mapB;
   rec.cb = &cb;
   std::vector<kdop::TestPair<V, K, T> > pool;
-  pool.push_back(kdop::TestPair<V, K, T>(ta, tb, pa->mesh, pb->mesh, pa->X, pb->X, pa->Y, pb->Y, pa->Z, pb->Z,
-                                         pa->surf, pb->surf, cb));
+  pool.push_back(kdop::TestPair<V, K, T>(ta, tb, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z, a.surf, b.surf, cb));
   g_tests = 0;
   g_recorder = &rec;
   kdop::tandem_traversal<V, K, T>(pool, kdop::sequential());
@@ -304,6 +361,7 @@ static int traverse_k(unsigned long long mem_bytes, int reorder, int nvA, float 
   return rec.missing ? -3 : 0;
 }
 #endif
+
 
 // Contacts of explicit tet pairs with the reference's MOST_OPPOSING_SURFACES
 // algorithm (geometry_contacts_tetrahedron_tetrahedron.h:1313-1345), in T.
@@ -341,30 +399,31 @@ static int contacts_pairs_t(float const* xyzA, unsigned const* tetsA, unsigned c
 }
 
 // ---- timing of the unmodified reference path --------------------------------
+// Untimed scene set-up: reorder, surface map and make_tree on the rest
+// positions of every mesh in use.  Timed, per mesh pair, the reference's
+// simulation-step hot path: rigid transform + refit_tree of both meshes
+// (narrow_update_kdop_bvh.h:146-171) and tandem_traversal with contact
+// generation (kdop_tandem_traversal.h:199-226).  Pairs run on `threads`
+// threads, one pair at a time per thread.
 template <size_t K>
-static int time_pairs_k(unsigned long long mem_bytes, int n_meshes, long long const* v_off,
-                        float const* xyz, long long const* t_off, unsigned const* tets, long long n_pairs,
-                        unsigned const* pairs, int threads, double* out_seconds, long long* out_contacts) {
+static int time_pairs_k(unsigned long long mem_bytes, int n_meshes, long long const* v_off, float const* xyz,
+                        float const* quat, float const* pos, long long const* t_off, unsigned const* tets,
+                        long long n_pairs, unsigned const* pairs, int threads, double* out_seconds,
+                        long long* out_contacts) {
   typedef float T;
   typedef tiny::MathTypes<T>::vector3_type V;
   std::vector<Mesh<T>*> meshes(n_meshes, (Mesh<T>*)0);
   std::vector<kdop::Tree<T, K>*> trees(n_meshes, (kdop::Tree<T, K>*)0);
   std::vector<char> used(n_meshes, 0);
   for (long long p = 0; p < n_pairs; ++p) used[pairs[2 * p]] = used[pairs[2 * p + 1]] = 1;
-  // scene setup (untimed): Morton reorder, surface map, tree build
   for (int m = 0; m < n_meshes; ++m) {
     if (!used[m]) continue;
-    Mesh<T> raw;
     int nv = (int)(v_off[m + 1] - v_off[m]);
     int nt = (int)(t_off[m + 1] - t_off[m]);
     std::vector<unsigned> lt(tets + 4 * t_off[m], tets + 4 * t_off[m + 1]);
-    make_mesh(raw, nv, xyz + 3 * v_off[m], nt, lt.data());
     meshes[m] = new Mesh<T>();
-    reorder_mesh(raw, *meshes[m]);
-    Mesh<T>& mm = *meshes[m];
-    mesh_array::compute_surface_map(mm.mesh, mm.X, mm.Y, mm.Z, mm.surf);
-    trees[m] = new kdop::Tree<T, K>(kdop::make_tree<V, K, T>((size_t)mem_bytes, mm.mesh, mm.X, mm.Y, mm.Z,
-                                                             kdop::sequential()));
+    trees[m] = new kdop::Tree<T, K>();
+    setup_mesh<T, K>(nv, xyz + 3 * v_off[m], nt, lt.data(), 1, mem_bytes, *meshes[m], *trees[m]);
   }
   if (threads < 1) threads = 1;
   std::vector<long long> contacts(threads, 0);
@@ -376,8 +435,9 @@ static int time_pairs_k(unsigned long long mem_bytes, int n_meshes, long long co
       unsigned ia = pairs[2 * p], ib = pairs[2 * p + 1];
       Mesh<T>& A = *meshes[ia];
       Mesh<T>& B = *meshes[ib];
-      // kdop_refit_tree.h:120 on both trees, then kdop_tandem_traversal.h:199
+      pose_mesh(A, quat + 4 * ia, pos + 3 * ia);
       kdop::refit_tree<V, K, T>(*trees[ia], A.mesh, A.X, A.Y, A.Z, kdop::sequential());
+      pose_mesh(B, quat + 4 * ib, pos + 3 * ib);
       kdop::refit_tree<V, K, T>(*trees[ib], B.mesh, B.X, B.Y, B.Z, kdop::sequential());
       CountCallback<T> cb;
       std::vector<kdop::TestPair<V, K, T> > pool;
@@ -445,15 +505,16 @@ int ref_mesh_reorder(int nv, float const* xyz, int nt, unsigned const* tets, flo
 
 // tiny::rotate(q, r) + p (narrow_update_kdop_bvh.h:160), q = (w, x, y, z).
 int ref_rotate(float const* q, float const* p, int nv, float const* xyz, float* out) {
-  typedef tiny::MathTypes<float> M;
-  M::quaternion_type Q(q[0], q[1], q[2], q[3]);
-  M::vector3_type P = M::vector3_type::make(p[0], p[1], p[2]);
+  refh::Mesh<float> m;
+  std::vector<unsigned> none(4, 0);
+  refh::make_mesh(m, nv, xyz, 0, none.data());
+  refh::keep_rest(m);
+  refh::pose_mesh(m, q, p);
   for (int i = 0; i < nv; ++i) {
-    M::vector3_type r0 = M::vector3_type::make(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
-    M::vector3_type r = tiny::rotate(Q, r0) + P;
-    out[3 * i] = r(0);
-    out[3 * i + 1] = r(1);
-    out[3 * i + 2] = r(2);
+    mesh_array::Vertex const& v = m.mesh.vertex(i);
+    out[3 * i] = m.X(v);
+    out[3 * i + 1] = m.Y(v);
+    out[3 * i + 2] = m.Z(v);
   }
   return 0;
 }
@@ -491,15 +552,16 @@ int ref_contacts_pairs(int fp64, float const* xyzA, unsigned const* tetsA, unsig
 }
 
 #if REF_RECORD
-int ref_traverse(int K, unsigned long long mem_bytes, int reorder, int nvA, float const* xyzA, int ntA,
-                 unsigned const* tetsA, int nvB, float const* xyzB, int ntB, unsigned const* tetsB,
-                 long long cap_pairs, unsigned* out_pairs, long long* out_npairs, long long cap_contacts,
-                 float* out_contacts, long long* out_ncontacts, long long* out_tests, long long cap_nodes,
-                 float* out_volsA, long long* out_leafA, long long* out_nnodesA) {
-#define REFH_TR(KK)                                                                                   \
-  case KK:                                                                                            \
-    return refh::traverse_k<KK>(mem_bytes, reorder, nvA, xyzA, ntA, tetsA, nvB, xyzB, ntB, tetsB,    \
-                                cap_pairs, out_pairs, out_npairs, cap_contacts, out_contacts,         \
+int ref_traverse(int K, unsigned long long mem_bytes, int reorder, int nvA, float const* restA, float const* qA,
+                 float const* pA, int ntA, unsigned const* tetsA, int nvB, float const* restB, float const* qB,
+                 float const* pB, int ntB, unsigned const* tetsB, long long cap_pairs, unsigned* out_pairs,
+                 long long* out_npairs, long long cap_contacts, float* out_contacts, long long* out_ncontacts,
+                 long long* out_tests, long long cap_nodes, float* out_volsA, long long* out_leafA,
+                 long long* out_nnodesA) {
+#define REFH_TR(KK)                                                                                      \
+  case KK:                                                                                               \
+    return refh::traverse_k<KK>(mem_bytes, reorder, nvA, restA, qA, pA, ntA, tetsA, nvB, restB, qB, pB, \
+                                ntB, tetsB, cap_pairs, out_pairs, out_npairs, cap_contacts, out_contacts,\
                                 out_ncontacts, out_tests, cap_nodes, out_volsA, out_leafA, out_nnodesA);
   switch (K) {
     REFH_TR(6) REFH_TR(8) REFH_TR(12) REFH_TR(14) REFH_TR(18) REFH_TR(20) REFH_TR(26)
@@ -510,12 +572,13 @@ int ref_traverse(int K, unsigned long long mem_bytes, int reorder, int nvA, floa
 #endif
 
 int ref_time_pairs(int K, unsigned long long mem_bytes, int n_meshes, long long const* v_off, float const* xyz,
-                   long long const* t_off, unsigned const* tets, long long n_pairs, unsigned const* pairs,
-                   int threads, double* out_seconds, long long* out_contacts) {
+                   float const* quat, float const* pos, long long const* t_off, unsigned const* tets,
+                   long long n_pairs, unsigned const* pairs, int threads, double* out_seconds,
+                   long long* out_contacts) {
 #define REFH_TP(KK)                                                                                  \
   case KK:                                                                                           \
-    return refh::time_pairs_k<KK>(mem_bytes, n_meshes, v_off, xyz, t_off, tets, n_pairs, pairs,     \
-                                  threads, out_seconds, out_contacts);
+    return refh::time_pairs_k<KK>(mem_bytes, n_meshes, v_off, xyz, quat, pos, t_off, tets, n_pairs,  \
+                                  pairs, threads, out_seconds, out_contacts);
   switch (K) {
     REFH_TP(6) REFH_TP(8) REFH_TP(12) REFH_TP(14) REFH_TP(18) REFH_TP(20) REFH_TP(26)
   }

@@ -1,0 +1,103 @@
+"""Generate tests/golden/*.npz from the reference's own CPU code.
+
+Run in a container where the reference sources are mounted and the harness is
+built (`make -C oracle ref REF_ROOT=<reference checkout>`):
+
+    python tests/golden/make_golden.py
+
+Every array comes out of oracle/_ref/libkdop_ref_record.so, i.e. the
+reference's make_tree / refit_tree / tandem_traversal / mesh_reorder /
+compute_surface_map / contacts_tetrahedron_tetrahedron / tiny::rotate compiled
+from its sources.  The fixtures pin the CPU oracle (oracle/kdop_oracle.c) and,
+through it, the CUDA library on machines where the reference is absent.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "bvh-tvcg18_b200"))
+
+from oracle.pyoracle import Reference  # noqa: E402
+from kdop_b200 import scenes  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def sha(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def sorted_pairs(p: np.ndarray) -> np.ndarray:
+    if p.size == 0:
+        return p.reshape(0, 2)
+    o = np.lexsort((p[:, 1], p[:, 0]))
+    return p[o]
+
+
+def main():
+    R = Reference()
+    g = {}
+    for K in scenes.SUPPORTED_K:
+        g[f"dirs_{K}"] = R.direction_table(K)
+
+    # rigid transform (tiny::rotate + translation)
+    rng = np.random.default_rng(123)
+    xyz = rng.uniform(-5, 5, size=(64, 3)).astype(np.float32)
+    q = scenes.random_quaternion(rng)
+    p = rng.uniform(-2, 2, size=3).astype(np.float32)
+    g["rotate_q"], g["rotate_p"], g["rotate_in"] = q, p, xyz
+    g["rotate_out"] = R.rotate(q, p, xyz)
+
+    # surface map and Morton order of a jittered 4^3 lattice
+    m = scenes.lattice(4, 0.2, np.random.default_rng(5))
+    g["lat4_xyz"], g["lat4_tets"] = m.xyz, m.tets
+    g["lat4_surf"] = R.surface_map(m.xyz, m.tets)
+    ox, ot = R.mesh_reorder(m.xyz, m.tets)
+    g["lat4_reorder_xyz"], g["lat4_reorder_tets"] = ox, ot
+
+    # config 1 (two 10^3 lattices, k = 14): pair list, node-pair tests, tree A
+    sc = scenes.config1()
+    A, B = sc.meshes
+    xa = R.rotate(sc.quat[0], sc.pos[0], A.xyz)
+    xb = R.rotate(sc.quat[1], sc.pos[1], B.xyz)
+    r = R.traverse(14, A.xyz, sc.quat[0], sc.pos[0], A.tets, B.xyz, sc.quat[1], sc.pos[1], B.tets,
+                   want_volumes=True)
+    g["c1_xyzB"] = xb
+    g["c1_pairs"] = sorted_pairs(r["pairs"])
+    g["c1_tests"] = np.int64(r["tests"])
+    g["c1_ncontacts"] = np.int64(len(r["contacts"]))
+    g["c1_volA_sha"] = np.array(sha(r["volumes"]))
+    g["c1_volA_head"] = r["volumes"][:64]
+    g["c1_leafA"] = r["leaf"]
+    r8 = R.traverse(14, A.xyz, sc.quat[0], sc.pos[0], A.tets, B.xyz, sc.quat[1], sc.pos[1], B.tets,
+                    mem_bytes=8000)
+    g["c1_chunked_pairs_sha"] = np.array(sha(sorted_pairs(r8["pairs"])))
+    g["c1_chunked_tests"] = np.int64(r8["tests"])
+
+    # contact-rich touching pairs, several K
+    for seed, K in [(0, 14), (1, 14), (2, 26), (3, 18), (4, 8)]:
+        sc = scenes.touching_pair(n=4, seed=seed, K=K)
+        A, B = sc.meshes
+        xa = R.rotate(sc.quat[0], sc.pos[0], A.xyz)
+        xb = R.rotate(sc.quat[1], sc.pos[1], B.xyz)
+        r = R.traverse(K, A.xyz, sc.quat[0], sc.pos[0], A.tets, B.xyz, sc.quat[1], sc.pos[1], B.tets)
+        key = f"t{seed}"
+        g[f"{key}_K"] = np.int64(K)
+        g[f"{key}_xyzA"], g[f"{key}_xyzB"] = xa, xb
+        g[f"{key}_pairs_trav"] = r["pairs"]
+        g[f"{key}_tests"] = np.int64(r["tests"])
+        g[f"{key}_contacts_f32"] = r["contacts"]
+        g[f"{key}_contacts_f64"] = R.contacts(xa, A.tets, A.surf, xb, B.tets, B.surf, r["pairs"], fp64=True)
+    np.savez_compressed(os.path.join(OUT, "reference_golden.npz"), **g)
+    print("wrote", os.path.join(OUT, "reference_golden.npz"), os.path.getsize(os.path.join(OUT, "reference_golden.npz")),
+          "bytes")
+
+
+if __name__ == "__main__":
+    main()

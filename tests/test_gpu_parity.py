@@ -1,0 +1,282 @@
+"""CUDA library (through its C ABI) against the CPU oracle / golden fixtures.
+
+Bars: node volumes, candidate pair sets and node-pair test counts bit-exact /
+exact; FP32 contacts bit-exact against the reference's FP32 path; contact
+depths and normals within 1e-5 relative of the FP64 oracle on pairs whose
+discrete decisions agree.
+"""
+import numpy as np
+import pytest
+
+import kdop_b200 as kd
+from conftest import sorted_rows, world_xyz
+from kdop_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_tree(oracle, K, rest, world, tets):
+    """Tree built on the rest positions, refitted on the world positions, in preorder."""
+    perm = oracle.morton_order(rest, tets)
+    left, right, tet = oracle.build_tree(perm)
+    vol = oracle.refit(K, world, tets, left, right, tet)
+    order, leaf = [], []
+    stack = [0]
+    while stack:
+        i = stack.pop()
+        order.append(i)
+        leaf.append(tet[i] if left[i] < 0 else -1)
+        if left[i] >= 0:
+            stack += [right[i], left[i]]
+    return vol[order], np.array(leaf)
+
+
+def scene_world(oracle, sc):
+    return [world_xyz(oracle, sc, i) for i in range(len(sc.meshes))]
+
+
+def oracle_pairs(oracle, sc, worlds, filt=True):
+    rows, tests = [], 0
+    for pi, (a, b) in enumerate(sc.pairs):
+        A, B = sc.meshes[a], sc.meshes[b]
+        sa = A.surf if filt else np.full(A.n_tets, 15, np.uint8)
+        sb = B.surf if filt else np.full(B.n_tets, 15, np.uint8)
+        p, t, _ = oracle.run_pair(sc.K, worlds[a], A.tets, sa, worlds[b], B.tets, sb, restA=A.xyz, restB=B.xyz)
+        tests += t
+        if len(p):
+            rows.append(np.column_stack([np.full(len(p), pi, np.uint32), p]))
+    rows = np.concatenate(rows) if rows else np.zeros((0, 3), np.uint32)
+    return sorted_rows(rows), tests
+
+
+@pytest.mark.parametrize("K", scenes.SUPPORTED_K)
+def test_refit_bit_exact_all_K(ctx, oracle, K):
+    rng = np.random.default_rng(K)
+    m = scenes.lattice(5, 0.2, rng)
+    q = scenes.random_quaternion(rng)
+    p = np.float32([0.5, -1.0, 2.0])
+    sc = kd.DeviceScene(ctx, K, [m])
+    # vertices mode
+    xw = oracle.rotate(q, p, m.xyz)
+    sc.set_vertices(xw)
+    sc.refit(kd.REFIT_VERTICES)
+    vol, tet = sc.read_tree(0)
+    ovol, oleaf = oracle_tree(oracle, K, m.xyz, xw, m.tets)
+    assert np.array_equal(tet, oleaf)
+    assert vol.tobytes() == ovol.tobytes()
+    # fused pose mode gives the same bits
+    sc.set_poses(q[None, :], p[None, :])
+    sc.refit(kd.REFIT_POSE)
+    vol2, _ = sc.read_tree(0)
+    assert vol2.tobytes() == ovol.tobytes()
+    assert sc.read_vertices().tobytes() == xw.tobytes()
+
+
+def test_refit_deform_mode_bit_exact(ctx, oracle):
+    m = scenes.lattice(4)
+    q = scenes.axis_angle_quaternion([1, 2, 3], 0.3)
+    p = np.float32([0.1, 0.2, 0.3])
+    sc = kd.DeviceScene(ctx, 18, [m])
+    sc.set_poses(q[None], p[None])
+    amp, w, phase = 0.1, np.float32(2 * np.pi / 4), 0.35
+    sc.set_deformation(amp, float(w), phase)
+    sc.refit(kd.REFIT_DEFORM)
+    xw = oracle.rotate(q, p, oracle.deform(amp, float(w), phase, m.xyz))
+    assert sc.read_vertices().tobytes() == xw.tobytes()
+    vol, _ = sc.read_tree(0)
+    ovol, _ = oracle_tree(oracle, 18, m.xyz, xw, m.tets)
+    assert vol.tobytes() == ovol.tobytes()
+
+
+def test_config1_against_golden(ctx, oracle, golden):
+    sc = scenes.config1()
+    ds = kd.DeviceScene(ctx, 14, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    for mode in (kd.TRAVERSE_BATCHED, kd.TRAVERSE_PLAIN):
+        st = ds.traverse_sync(sc.pairs, ds.opts(mode=mode))
+        rows = ds.candidates()
+        assert np.array_equal(sorted_rows(rows[:, 1:]), golden["c1_pairs"])
+        assert st.n_tests == int(golden["c1_tests"])
+    vol, tet = ds.read_tree(0)
+    assert np.array_equal(tet, golden["c1_leafA"])
+    assert vol[:64].tobytes() == golden["c1_volA_head"].tobytes()
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 4])
+def test_touching_pairs_contacts_bit_exact(ctx, oracle, golden, seed):
+    key = f"t{seed}"
+    K = int(golden[f"{key}_K"])
+    sc = scenes.touching_pair(n=4, seed=seed, K=K)
+    ds = kd.DeviceScene(ctx, K, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    st = ds.traverse_sync(sc.pairs, contacts=True)
+    assert st.n_tests == int(golden[f"{key}_tests"])
+    rows = ds.candidates()
+    ref_pairs = golden[f"{key}_pairs_trav"]
+    assert np.array_equal(sorted_rows(rows[:, 1:]), sorted_rows(ref_pairs))
+    # contacts: group the device rows by candidate, order candidates as the
+    # reference's traversal visited them, then compare bit for bit
+    c = ds.read_contacts()
+    cand = rows[c["cand"], 1:]
+    index = {(int(a), int(b)): i for i, (a, b) in enumerate(ref_pairs)}
+    order = np.array([index[(int(a), int(b))] for a, b in cand])
+    perm = np.lexsort((np.arange(len(c)), order))
+    dev = np.column_stack([c["p"], c["n"], c["depth"][:, None], order[:, None].astype(np.float32)])[perm]
+    ref = golden[f"{key}_contacts_f32"]
+    assert dev.shape == ref.shape
+    assert dev.tobytes() == ref.tobytes()
+    # FP64 oracle: depths and normals within 1e-5 relative where decisions agree
+    r64 = golden[f"{key}_contacts_f64"]
+    groups32 = {}
+    for row in ref:
+        groups32.setdefault(int(row[7]), []).append(row)
+    groups64 = {}
+    for row in r64:
+        groups64.setdefault(int(row[7]), []).append(row)
+    agree = 0
+    for pid, g32 in groups32.items():
+        g64 = groups64.get(pid)
+        if g64 is None or len(g64) != len(g32):
+            continue
+        a, b = np.array(g32), np.array(g64)
+        if not np.allclose(a[:, 3:6], b[:, 3:6], rtol=0, atol=1e-3):
+            continue
+        agree += 1
+        scale = max(1.0, np.abs(b[:, 6]).max())
+        assert np.abs(a[:, 6] - b[:, 6]).max() <= 1e-5 * scale
+        assert np.abs(a[:, 3:6] - b[:, 3:6]).max() <= 1e-5
+    assert agree >= 0.9 * len(groups32)
+
+
+@pytest.mark.parametrize("K", [6, 14, 26])
+def test_small_batch_batched_equals_plain_equals_oracle(ctx, oracle, K):
+    sc = scenes.small_batch(n_pairs=12, seed=K, K=K)
+    worlds = scene_world(oracle, sc)
+    ds = kd.DeviceScene(ctx, K, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    ref_rows, ref_tests = oracle_pairs(oracle, sc, worlds)
+    # the reference counts one root test per pair and then tests the root pair
+    # again in the recursion; the oracle does the same
+    for mode in (kd.TRAVERSE_BATCHED, kd.TRAVERSE_PLAIN):
+        st = ds.traverse_sync(sc.pairs, ds.opts(mode=mode))
+        assert st.n_tests == ref_tests
+        assert np.array_equal(sorted_rows(ds.candidates()), ref_rows)
+
+
+def test_surface_filter_off_matches_unfiltered_oracle(ctx, oracle):
+    sc = scenes.small_batch(n_pairs=6, seed=3)
+    worlds = scene_world(oracle, sc)
+    ds = kd.DeviceScene(ctx, 14, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    st = ds.traverse_sync(sc.pairs, ds.opts(surface_filter=0))
+    ref_rows, _ = oracle_pairs(oracle, sc, worlds, filt=False)
+    assert st.n_leaf_overlaps == len(ref_rows) == st.n_candidates
+    assert np.array_equal(sorted_rows(ds.candidates()), ref_rows)
+
+
+@pytest.mark.parametrize("cfg", [dict(block_warps=4, stack_cap=64, donate_min=8),
+                                 dict(block_warps=16, stack_cap=1024, init_chunk=4, donate_min=128),
+                                 dict(block_warps=2, stack_cap=128, init_chunk=32, donate_min=16)])
+def test_tuning_knobs_do_not_change_results(ctx, oracle, cfg):
+    sc = scenes.small_batch(n_pairs=10, n_lo=3, n_hi=7, seed=21)
+    worlds = scene_world(oracle, sc)
+    ds = kd.DeviceScene(ctx, 14, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    ref_rows, ref_tests = oracle_pairs(oracle, sc, worlds)
+    st = ds.traverse_sync(sc.pairs, ds.opts(**cfg))
+    assert st.n_tests == ref_tests
+    assert np.array_equal(sorted_rows(ds.candidates()), ref_rows)
+
+
+def test_capacity_overflow_reports_and_retries(ctx, oracle):
+    sc = scenes.small_batch(n_pairs=4, seed=9)
+    ds = kd.DeviceScene(ctx, 14, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    ds.traverse(sc.pairs)
+    full = ds.stats()
+    assert full.n_candidates > 16
+    rows = sorted_rows(ds.candidates())
+    # tiny candidate and queue buffers: the call reports the required size
+    ds.set_capacity(candidates=8, queue=2)
+    ds.traverse(sc.pairs, ds.opts(stack_cap=64, donate_min=8))
+    st = ds.stats(check=False)
+    assert st.status == kd.lib.ERR_CAPACITY
+    assert st.n_candidates == full.n_candidates or st.device_error & 2
+    st = ds.traverse_sync(sc.pairs, ds.opts(stack_cap=64, donate_min=8), max_retries=12)
+    assert st.n_candidates == full.n_candidates and st.n_tests == full.n_tests
+    assert np.array_equal(sorted_rows(ds.candidates()), rows)
+
+
+def test_contact_capacity_overflow(ctx):
+    sc = scenes.touching_pair(n=3, seed=1)
+    ds = kd.DeviceScene(ctx, 14, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    st = ds.traverse_sync(sc.pairs, contacts=True)
+    ref = ds.read_contacts()
+    assert st.n_contacts > 8
+    ds.set_capacity(contacts=4)
+    ds.traverse(sc.pairs)
+    ds.contacts()
+    st2 = ds.stats(check=False)
+    assert st2.status == kd.lib.ERR_CAPACITY and st2.n_contacts == st.n_contacts
+    ds.traverse_sync(sc.pairs, contacts=True)
+    got = ds.read_contacts()
+    assert len(got) == len(ref)
+
+
+def test_edge_cases_empty_and_single_tet(ctx, oracle):
+    one = scenes.Mesh(np.float32([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]]), np.uint32([[0, 1, 2, 3]]),
+                      np.uint8([15]))
+    empty = scenes.Mesh(np.zeros((0, 3), np.float32), np.zeros((0, 4), np.uint32), np.zeros(0, np.uint8))
+    big = scenes.lattice(2)
+    ds = kd.DeviceScene(ctx, 14, [one, empty, big, one])
+    xyz = np.concatenate([one.xyz, empty.xyz, big.xyz - 0.5, one.xyz + np.float32([0.25, 0.25, 0.25])])
+    ds.set_vertices(xyz)
+    ds.refit(kd.REFIT_VERTICES)
+    # no pairs at all
+    st = ds.traverse_sync(np.zeros((0, 2), np.uint32))
+    assert st.n_tests == 0 and st.n_candidates == 0
+    # empty mesh pairs do nothing; leaf-leaf roots; leaf vs tree
+    pairs = np.uint32([[0, 1], [1, 2], [0, 3], [3, 2], [2, 0]])
+    st = ds.traverse_sync(pairs)
+    rows = sorted_rows(ds.candidates())
+    ref = []
+    tests = 0
+    meshes = [one, empty, big, one]
+    offs = np.cumsum([0] + [m.n_verts for m in meshes])
+    for pi, (a, b) in enumerate(pairs):
+        A, B = meshes[a], meshes[b]
+        if A.n_tets == 0 or B.n_tets == 0:
+            continue
+        p, t, _ = oracle.run_pair(14, xyz[offs[a]:offs[a + 1]], A.tets, A.surf, xyz[offs[b]:offs[b + 1]], B.tets,
+                                  B.surf, restA=A.xyz, restB=B.xyz)
+        tests += t
+        ref += [(pi, x, y) for x, y in p]
+    assert st.n_tests == tests
+    assert np.array_equal(rows, sorted_rows(np.array(ref, np.uint32).reshape(-1, 3)))
+
+
+def test_invalid_arguments_are_errors_not_crashes(ctx):
+    m = scenes.lattice(1)
+    with pytest.raises(kd.KdopError):
+        kd.DeviceScene(ctx, 10, [m])  # unsupported K
+    bad = scenes.Mesh(m.xyz, m.tets.copy(), m.surf)
+    bad.tets[0, 0] = 999
+    with pytest.raises(kd.KdopError):
+        kd.DeviceScene(ctx, 14, [bad])
+    ds = kd.DeviceScene(ctx, 14, [m, m])
+    with pytest.raises(kd.KdopError):
+        ds.traverse(np.uint32([[0, 5]]))  # mesh index out of range
+    with pytest.raises(kd.KdopError):
+        ds.set_vertices(np.zeros((3, 3), np.float32))  # wrong vertex count
+    with pytest.raises(kd.KdopError):
+        ds.refit(7)
+    with pytest.raises(kd.KdopError):
+        ds.traverse(np.uint32([[0, 1]]), ds.opts(stack_cap=100))  # not a power of two

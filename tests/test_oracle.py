@@ -1,0 +1,108 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures made by
+tests/golden/make_golden.py from the reference's compiled CPU path) and, where
+the reference harness is built, against the reference directly."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import sorted_rows, world_xyz
+from kdop_b200 import scenes
+
+
+def preorder(left, right, tet, vol):
+    order, leaf = [], []
+    stack = [0]
+    while stack:
+        i = stack.pop()
+        order.append(i)
+        leaf.append(tet[i] if left[i] < 0 else -1)
+        if left[i] >= 0:
+            stack.append(right[i])
+            stack.append(left[i])
+    return vol[order], np.array(leaf)
+
+
+@pytest.mark.parametrize("K", scenes.SUPPORTED_K)
+def test_direction_tables_bit_exact(oracle, golden, K):
+    assert oracle.dirs(K).tobytes() == golden[f"dirs_{K}"].tobytes()
+
+
+def test_rotate_bit_exact(oracle, golden):
+    out = oracle.rotate(golden["rotate_q"], golden["rotate_p"], golden["rotate_in"])
+    assert out.tobytes() == golden["rotate_out"].tobytes()
+
+
+def test_surface_map(oracle, golden):
+    tets = golden["lat4_tets"]
+    assert np.array_equal(oracle.surface_map(golden["lat4_xyz"].shape[0], tets), golden["lat4_surf"])
+    assert np.array_equal(scenes.surface_map(tets), golden["lat4_surf"])
+
+
+def test_morton_order_matches_reference_reorder(oracle, golden):
+    xyz, tets = golden["lat4_xyz"], golden["lat4_tets"]
+    perm = oracle.morton_order(xyz, tets)
+    mine = xyz[tets[perm]].reshape(-1, 12)
+    ref = golden["lat4_reorder_xyz"][golden["lat4_reorder_tets"]].reshape(-1, 12)
+    assert np.array_equal(mine, ref)
+
+
+def test_config1_pairs_tests_and_tree(oracle, golden):
+    sc = scenes.config1()
+    A, B = sc.meshes
+    xb = world_xyz(oracle, sc, 1)
+    assert xb.tobytes() == golden["c1_xyzB"].tobytes()
+    xa = world_xyz(oracle, sc, 0)
+    pairs, tests, _ = oracle.run_pair(14, xa, A.tets, A.surf, xb, B.tets, B.surf, restA=A.xyz, restB=B.xyz)
+    assert np.array_equal(sorted_rows(pairs), golden["c1_pairs"])
+    assert tests == int(golden["c1_tests"])
+    # whole tree of A: node volumes in preorder, bit for bit
+    perm = oracle.morton_order(A.xyz, A.tets)
+    left, right, tet = oracle.build_tree(perm)
+    vol = oracle.refit(14, xa, A.tets, left, right, tet)
+    pv, leaf = preorder(left, right, tet, vol)
+    assert hashlib.sha256(pv.tobytes()).hexdigest() == str(golden["c1_volA_sha"])
+    assert np.array_equal(leaf, golden["c1_leafA"])
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 4])
+def test_touching_pairs_contacts(oracle, golden, seed):
+    key = f"t{seed}"
+    K = int(golden[f"{key}_K"])
+    sc = scenes.touching_pair(n=4, seed=seed, K=K)
+    A, B = sc.meshes
+    xa, xb = golden[f"{key}_xyzA"], golden[f"{key}_xyzB"]
+    assert world_xyz(oracle, sc, 1).tobytes() == xb.tobytes()
+    pairs, tests, _ = oracle.run_pair(K, xa, A.tets, A.surf, xb, B.tets, B.surf, restA=A.xyz, restB=B.xyz)
+    # same traversal order as the reference's recursion
+    assert np.array_equal(pairs, golden[f"{key}_pairs_trav"])
+    assert tests == int(golden[f"{key}_tests"])
+    cf, _ = oracle.contacts(xa, A.tets, A.surf, xb, B.tets, B.surf, pairs, "f")
+    assert len(cf) > 0
+    assert cf.tobytes() == golden[f"{key}_contacts_f32"].tobytes()
+    cd, _ = oracle.contacts(xa, A.tets, A.surf, xb, B.tets, B.surf, pairs, "d")
+    assert np.array_equal(cd, golden[f"{key}_contacts_f64"])
+
+
+def test_sine_accuracy(oracle):
+    xs = np.linspace(-40.0, 40.0, 2001, dtype=np.float32)
+    ys = np.array([oracle.sin(float(x)) for x in xs])
+    assert np.max(np.abs(ys - np.sin(xs.astype(np.float64)))) < 2e-6
+
+
+@pytest.mark.parametrize("K,seed", [(6, 1), (8, 2), (12, 3), (14, 4), (18, 5), (20, 6), (26, 7)])
+def test_oracle_against_reference_random(oracle, reference, K, seed):
+    rng = np.random.default_rng(seed)
+    a = scenes.lattice(int(rng.integers(2, 5)), 0.15, rng)
+    b = scenes.lattice(int(rng.integers(2, 5)), 0.15, rng)
+    q = scenes.random_quaternion(rng)
+    p = rng.uniform(-1.5, 1.5, size=3).astype(np.float32)
+    xb = oracle.rotate(q, p, b.xyz)
+    assert xb.tobytes() == reference.rotate(q, p, b.xyz).tobytes()
+    q0, p0 = np.float32([1, 0, 0, 0]), np.float32([0, 0, 0])
+    r = reference.traverse(K, a.xyz, q0, p0, a.tets, b.xyz, q, p, b.tets)
+    pairs, tests, _ = oracle.run_pair(K, a.xyz, a.tets, a.surf, xb, b.tets, b.surf, restA=a.xyz, restB=b.xyz)
+    assert np.array_equal(pairs, r["pairs"])
+    assert tests == r["tests"]
+    cf, _ = oracle.contacts(a.xyz, a.tets, a.surf, xb, b.tets, b.surf, pairs, "f")
+    assert cf.tobytes() == r["contacts"].tobytes()
