@@ -1,0 +1,431 @@
+"""Benchmark of the kDOP BVH collision step on B200.
+
+Workload (default): the batched configuration -- 512 mesh pairs of uneven size
+(1k-200k tets per mesh, log-uniform), jittered Kuhn lattices, random rigid
+poses, k = 14.  One step = the reference's per-step hot path for all pairs:
+rigid transform + kDOP refit of every mesh, tandem traversal of every pair
+(one persistent launch), MOST_OPPOSING contact generation; captured in one
+CUDA graph.  Metric: kDOP node-pair tests per second (the reference's
+overlap_dop_dop calls, counted exactly as the reference counts them).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+N > 1 runs under torch.distributed (one rank per GPU); every rank processes
+its own 512-pair batch (weak scaling, no data exchange); the step time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "bvh-tvcg18_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "kDOP tandem-traversal node-pair tests/s, batched vs plain, % of HBM roofline"
+UNIT = "node-pair tests/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--pairs", type=int, default=512)
+    ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample, seconds")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    return ap.parse_args()
+
+
+# ---- distributed plumbing -------------------------------------------------------
+class Dist:
+    def __init__(self, backend: str):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            if self.pg.get_backend() == "nccl":
+                import torch
+                self.pg.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---- clocks during the timed region ----------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(name: str):
+    """dram bytes per launch from a committed ncu summary (profiles/<name>.md)."""
+    path = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_full_launch\s*=\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def workload(args, rank: int):
+    from kdop_b200 import scenes
+    return scenes.config3(n_pairs=args.pairs, seed=2 + rank)
+
+
+def cpu_sample(sc, tests_per_pair, budget_tests):
+    """First pairs of the workload whose node-pair tests sum to the budget."""
+    n, acc = 0, 0
+    for t in tests_per_pair:
+        if n > 0 and acc + t > budget_tests:
+            break
+        acc += int(t)
+        n += 1
+    return n, acc
+
+
+def oracle_tests_per_pair(sc, threads=0):
+    from oracle.pyoracle import Oracle
+    O = Oracle()
+    worlds = [O.rotate(sc.quat[i], sc.pos[i], m.xyz) for i, m in enumerate(sc.meshes)]
+    _, tpp, _ = O.run_pairs(sc.K, worlds, sc.meshes, sc.pairs, threads=threads)
+    return tpp
+
+
+def reference_time(sc, n_pairs, threads):
+    from oracle.pyoracle import RefTimer
+    R = RefTimer()
+    used = sorted(set(sc.pairs[:n_pairs].ravel().tolist()))
+    remap = {m: i for i, m in enumerate(used)}
+    meshes = [sc.meshes[m] for m in used]
+    pairs = np.array([[remap[a], remap[b]] for a, b in sc.pairs[:n_pairs]], np.uint32)
+    sec, contacts = R.time_pairs(sc.K, meshes, sc.quat[used], sc.pos[used], pairs, threads=threads)
+    return sec, contacts
+
+
+# ---- reference arm ----------------------------------------------------------------
+def run_reference(args):
+    dist = Dist("gloo")
+    if dist.rank != 0:
+        dist.close()
+        return
+    from oracle import pyoracle
+    if not pyoracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU path not built (oracle/_ref missing)"}))
+        return
+    threads = os.cpu_count() or 1
+    sc = workload(args, 0)
+    tpp = oracle_tests_per_pair(sc)
+    # per step: a bounded sample of the workload, sized for ~4 s on all threads
+    n, tests = cpu_sample(sc, tpp, budget_tests=4.0 * 30e6 * threads)
+    times = []
+    for i in range(args.warmup + args.steps):
+        sec, _ = reference_time(sc, n, threads)
+        if i >= args.warmup:
+            times.append(sec)
+    t = sum(times) / len(times)
+    value = tests / t
+    sample = f"first {n} of {len(sc.pairs)} pairs per step ({tests} node-pair tests)"
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": sc.name, "pairs": int(len(sc.pairs)), "K": sc.K,
+                       "sample_pairs": n, "threads": threads},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---- CUDA arm -------------------------------------------------------------------------
+def run_cuda(args):
+    import torch
+
+    import kdop_b200 as kd
+
+    dist = Dist("nccl")
+    torch.cuda.set_device(dist.local)
+    sc = workload(args, dist.rank)
+    ctx = kd.Context(dist.local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    info = ds.info()
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    st = ds.traverse_sync(sc.pairs, contacts=True)
+    tuned = None
+    if not args.no_autotune:
+        tuned = ds.autotune(sc.pairs, repeats=2).as_dict()
+    opts = ds.default_opts()
+    st = ds.traverse_sync(sc.pairs, opts, contacts=True)
+    tests_per_step = st.n_tests
+    ds.reserve(candidates=int(st.n_candidates * 1.2) + 1024, contacts=int(st.n_contacts * 1.2) + 1024,
+               queue=max(st.queue_used * 2, 1 << 20))
+
+    # one step = motion-free pose refit + traversal + contacts in one CUDA graph
+    ds.graph_capture(sc.pairs, refit_mode=kd.REFIT_POSE, opts=opts)
+    launches0 = ctx.launches
+    for _ in range(args.warmup):
+        ds.graph_launch()
+    ctx.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    launches_before = ctx.launches
+    e0.record(stream)
+    for _ in range(args.steps):
+        ds.graph_launch()
+    e1.record(stream)
+    e1.synchronize()
+    launches_timed = ctx.launches - launches_before
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    dist.barrier()
+    st2 = ds.stats()
+    assert st2.n_tests == tests_per_step, (st2.n_tests, tests_per_step)
+    ms_max = dist.max(ms)
+    total_tests = dist.sum(float(tests_per_step))
+    value = total_tests / (ms_max * 1e-3)
+
+    # dominant kernel: the batched traversal launch, timed alone
+    reps = 5
+    tt = []
+    for _ in range(reps + 1):
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        ds.traverse(sc.pairs, opts)
+        a1.record(stream)
+        a1.synchronize()
+        tt.append(a0.elapsed_time(a1))
+    trav_ms = statistics.median(tt[1:])
+    node_bytes = info["node_bytes"]
+    alg_bytes = tests_per_step * 2 * node_bytes
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (trav_ms * 1e-3) / 1e9
+    traffic = ncu_traffic("traverse_config3.md")
+
+    # plain: one traversal launch per mesh pair, same trees and descent rule
+    plain = None
+    if not args.no_plain:
+        popts = ds.opts(mode=kd.TRAVERSE_PLAIN)
+        ds.traverse_sync(sc.pairs, popts)
+        pt = []
+        for _ in range(2):
+            a0 = torch.cuda.Event(enable_timing=True)
+            a1 = torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            ds.traverse(sc.pairs, popts)
+            a1.record(stream)
+            a1.synchronize()
+            pt.append(a0.elapsed_time(a1))
+        pst = ds.stats()
+        assert pst.n_tests == tests_per_step
+        plain_ms = min(pt)
+        plain = {"traversal_ms": plain_ms, "tests_per_s": tests_per_step / (plain_ms * 1e-3),
+                 "batched_speedup": plain_ms / trav_ms}
+
+    # e2e: through the public API with host buffers; per step the world
+    # positions of all meshes go host->device (pinned) and the contacts and
+    # counters come back device->host
+    from oracle.pyoracle import Oracle
+    O = Oracle()
+    world = np.concatenate([O.rotate(sc.quat[i], sc.pos[i], m.xyz) for i, m in enumerate(sc.meshes)])
+    h_xyz = torch.empty((world.shape[0], 3), dtype=torch.float32, pin_memory=True)
+    h_xyz.numpy()[:] = world
+    h_pairs = torch.empty((len(sc.pairs), 2), dtype=torch.int32, pin_memory=True)
+    h_pairs.numpy()[:] = sc.pairs.astype(np.int32)
+    n_cont_cap = ds.stats().contact_capacity
+    h_cont = torch.empty((n_cont_cap * 8,), dtype=torch.float32, pin_memory=True)
+    import ctypes
+
+    def e2e_step():
+        ds.set_vertices(h_xyz.numpy())
+        ds.refit(kd.REFIT_VERTICES)
+        ds.traverse(h_pairs.numpy().view(np.uint32), opts)
+        ds.contacts()
+        s = ds.stats()
+        n = C_n = ctypes.c_int64()
+        ds.ctx._check(ds.lib.kdop_read_contacts(ds.h, ctypes.c_void_p(h_cont.data_ptr()), n_cont_cap,
+                                                ctypes.byref(C_n)))
+        return s, n.value
+
+    for _ in range(2):
+        e2e_step()
+    ctx.synchronize()
+    dist.barrier()
+    w0 = time.perf_counter()
+    b0 = torch.cuda.Event(enable_timing=True)
+    b1 = torch.cuda.Event(enable_timing=True)
+    b0.record(stream)
+    ncont = 0
+    for _ in range(args.e2e_steps):
+        s, ncont = e2e_step()
+    b1.record(stream)
+    b1.synchronize()
+    e2e_ms = max(b0.elapsed_time(b1), (time.perf_counter() - w0) * 1e3) / args.e2e_steps
+    assert s.n_tests == tests_per_step
+    e2e_ms_max = dist.max(e2e_ms)
+    e2e_value = total_tests / (e2e_ms_max * 1e-3)
+    h2d = world.nbytes + sc.pairs.nbytes
+    d2h = ncont * 32 + 128
+
+    # CPU baseline: the reference's own CPU path, one thread, bounded sample
+    cpu = None
+    if dist.rank == 0 and not args.no_cpu_baseline:
+        from oracle import pyoracle
+        if pyoracle.reference_available():
+            tpp = oracle_tests_per_pair(sc)
+            n, tests = cpu_sample(sc, tpp, budget_tests=args.cpu_seconds * 30e6)
+            sec, _ = reference_time(sc, n, 1)
+            cpu = {"value": tests / sec, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": f"first {n} of {len(sc.pairs)} pairs, one step ({tests} node-pair tests, "
+                             f"{sec:.1f} s), rigid transform + refit + tandem traversal with contacts"}
+        else:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": "unavailable: oracle/_ref not built"}
+
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": sc.name, "pairs_per_gpu": int(len(sc.pairs)), "tets_per_gpu": int(sc.n_tets),
+                       "K": sc.K, "node_bytes": node_bytes, "parallelism": f"pairs sharded, {dist.world} rank(s)",
+                       "l2": f"inputs larger than L2 (node records {info['n_nodes'] * node_bytes / 1e9:.2f} GB)",
+                       "step": "CUDA graph: pose transform + refit, batched traversal, contacts",
+                       "tests_per_step_per_gpu": int(tests_per_step), "candidates": int(st2.n_candidates),
+                       "contacts": int(st2.n_contacts), "traverse_opts": opts.as_dict(), "autotuned": tuned},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "traverse_kernel (batched, one persistent launch)",
+                         "launch_ms": trav_ms, "algorithmic_bytes_per_launch": alg_bytes},
+            "plain": plain,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": e2e_ms_max},
+            "gpu_launches": int(launches_timed),
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    ds.graph_release()
+    ds.close()
+    ctx.close()
+    dist.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -150,11 +150,20 @@ int kdop_ctx_create(int device, kdop_ctx** out) {
   return KDOP_OK;
 }
 
-int kdop_ctx_destroy(kdop_ctx* ctx) {
-  if (!ctx) return KDOP_ERR_INVALID;
+static void ctx_free(kdop_ctx* ctx) {
   cudaSetDevice(ctx->device);
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
+}
+
+int kdop_ctx_destroy(kdop_ctx* ctx) {
+  if (!ctx || ctx->destroy_pending) return KDOP_ERR_INVALID;
+  // scenes keep using the context's stream: free it with the last scene
+  if (ctx->n_scenes > 0) {
+    ctx->destroy_pending = true;
+    return KDOP_OK;
+  }
+  ctx_free(ctx);
   return KDOP_OK;
 }
 
@@ -399,16 +408,19 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
     delete box;
     return rc;
   }
+  ctx->n_scenes++;
   *out = s;
   return KDOP_OK;
 }
 
 int kdop_scene_destroy(kdop_scene* s) {
   if (!s) return KDOP_ERR_INVALID;
-  cudaSetDevice(s->ctx->device);
-  cudaStreamSynchronize(s->ctx->stream);
+  kdop_ctx* ctx = s->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
   scene_free(s);
   delete reinterpret_cast<SceneBox*>(s);
+  if (--ctx->n_scenes == 0 && ctx->destroy_pending) ctx_free(ctx);
   return KDOP_OK;
 }
 

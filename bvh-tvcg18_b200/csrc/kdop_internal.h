@@ -63,6 +63,9 @@ struct kdop_ctx {
   size_t smem_optin = 0;
   std::string err;
   long long launches = 0;
+  // scenes alive on this context; a destroyed context is freed with its last scene
+  int n_scenes = 0;
+  bool destroy_pending = false;
   // autotuned traversal options keyed by (K, size class)
   std::map<std::pair<int, int>, kdop_traverse_opts> tuned;
 };

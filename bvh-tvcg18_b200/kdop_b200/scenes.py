@@ -59,21 +59,57 @@ class Scene:
         return sum(m.n_tets for m in self.meshes)
 
 
+_TOPOLOGY = {}
+
+
+def lattice_topology(n: int):
+    """(rest xyz float64, tets, surface map) of the n^3-cell lattice, cached."""
+    if n not in _TOPOLOGY:
+        m = n + 1
+        g = np.arange(m, dtype=np.float64)
+        z, y, x = np.meshgrid(g, g, g, indexing="ij")
+        xyz = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1) - n / 2.0
+        ci = np.arange(n)
+        ck, cj, cii = np.meshgrid(ci, ci, ci, indexing="ij")
+        base = (cii + m * (cj + m * ck)).ravel()
+        corner = np.array([(c & 1) + m * ((c >> 1) & 1) + m * m * ((c >> 2) & 1) for c in range(8)])
+        tets = (base[:, None, None] + corner[KUHN][None, :, :]).reshape(-1, 4).astype(np.uint32)
+        for a in (xyz, tets):
+            a.setflags(write=False)
+        surf = _lattice_surface(n, tets)
+        surf.setflags(write=False)
+        _TOPOLOGY[n] = (xyz, tets, surf)
+    return _TOPOLOGY[n]
+
+
+def _lattice_surface(n: int, tets: np.ndarray) -> np.ndarray:
+    # boundary faces of the Kuhn lattice: a face is on the boundary iff its
+    # three vertices lie on one face of the cube [0, n]^3 (a face strictly
+    # inside the cube always has a second tet); checked against face counting
+    # in the tests.
+    if n <= 8:
+        return surface_map(tets)
+    m = n + 1
+    v = tets.astype(np.int64)
+    coords = np.stack([v % m, (v // m) % m, v // (m * m)], axis=-1)  # (nt, 4, 3)
+    surf = np.zeros(tets.shape[0], np.uint8)
+    for k in range(4):
+        others = [u for u in range(4) if u != k]
+        c = coords[:, others, :]  # (nt, 3, 3)
+        on = np.zeros(tets.shape[0], bool)
+        for d in range(3):
+            col = c[:, :, d]
+            on |= np.all(col == 0, axis=1) | np.all(col == n, axis=1)
+        surf |= on.astype(np.uint8) << k
+    return surf
+
+
 def lattice(n: int, jitter: float = 0.0, rng: Optional[np.random.Generator] = None) -> Mesh:
     """n^3 cubes x 6 Kuhn tets, centred on the origin, optional uniform jitter."""
-    m = n + 1
-    g = np.arange(m, dtype=np.float64)
-    z, y, x = np.meshgrid(g, g, g, indexing="ij")
-    xyz = np.stack([x.ravel(), y.ravel(), z.ravel()], axis=1) - n / 2.0
+    xyz, tets, surf = lattice_topology(n)
     if jitter:
         xyz = xyz + rng.uniform(-jitter, jitter, size=xyz.shape)
-    ci = np.arange(n)
-    ck, cj, cii = np.meshgrid(ci, ci, ci, indexing="ij")
-    base = (cii + m * (cj + m * ck)).ravel()
-    corner = np.array([(c & 1) + m * ((c >> 1) & 1) + m * m * ((c >> 2) & 1) for c in range(8)])
-    tets = (base[:, None, None] + corner[KUHN][None, :, :]).reshape(-1, 4)
-    tets = tets.astype(np.uint32)
-    return Mesh(xyz.astype(np.float32), tets, surface_map(tets))
+    return Mesh(xyz.astype(np.float32), tets, surf)
 
 
 def surface_map(tets: np.ndarray) -> np.ndarray:

@@ -36,6 +36,7 @@ typedef struct {
   int32_t imax;    /* candidate code attaining max p.n */
   int32_t ncontacts; /* unique contacts reported */
   int32_t overlap; /* exact tet-tet SAT overlap */
+  uint64_t cand_mask; /* bit c set: contact candidate c was generated */
 } or_record;
 
 int or_dirs_f(int K, float* out);

@@ -280,6 +280,7 @@ static int F(pair_contacts)(const F(v3)* A, const F(v3)* B, unsigned sa, unsigne
   rec->imin = rec->imax = -1;
   rec->ncontacts = 0;
   rec->overlap = 0;
+  rec->cand_mask = 0;
   if (!sa || !sb) return 0;
   if (!F(tet_overlap)(A, B)) return 0;
   rec->overlap = 1;
@@ -297,7 +298,10 @@ static int F(pair_contacts)(const F(v3)* A, const F(v3)* B, unsigned sa, unsigne
   int code[OR_NCAND];
   int nq = 0;
   for (int c = 0; c < OR_NCAND; ++c)
-    if (F(candidate)(c, A, B, PA, PB, &q[nq])) code[nq++] = c;
+    if (F(candidate)(c, A, B, PA, PB, &q[nq])) {
+      rec->cand_mask |= 1ull << c;
+      code[nq++] = c;
+    }
   if (!nq) return 0;
   REAL big = (sizeof(REAL) == 4) ? (REAL)FLT_MAX : (REAL)DBL_MAX;
   REAL mn = big, mx = -big;

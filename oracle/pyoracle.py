@@ -34,11 +34,12 @@ def _c(a, dtype):
 
 class OrRecord(C.Structure):
     _fields_ = [("face_a", C.c_int32), ("face_b", C.c_int32), ("imin", C.c_int32), ("imax", C.c_int32),
-                ("ncontacts", C.c_int32), ("overlap", C.c_int32)]
+                ("ncontacts", C.c_int32), ("overlap", C.c_int32), ("cand_mask", C.c_uint64)]
 
 
 OR_RECORD_DTYPE = np.dtype([("face_a", np.int32), ("face_b", np.int32), ("imin", np.int32),
-                            ("imax", np.int32), ("ncontacts", np.int32), ("overlap", np.int32)])
+                            ("imax", np.int32), ("ncontacts", np.int32), ("overlap", np.int32),
+                            ("cand_mask", np.uint64)])
 
 
 def available() -> bool:

@@ -127,27 +127,46 @@ def test_touching_pairs_contacts_bit_exact(ctx, oracle, golden, seed):
     ref = golden[f"{key}_contacts_f32"]
     assert dev.shape == ref.shape
     assert dev.tobytes() == ref.tobytes()
-    # FP64 oracle: depths and normals within 1e-5 relative where decisions agree
-    r64 = golden[f"{key}_contacts_f64"]
-    groups32 = {}
-    for row in ref:
-        groups32.setdefault(int(row[7]), []).append(row)
-    groups64 = {}
-    for row in r64:
-        groups64.setdefault(int(row[7]), []).append(row)
-    agree = 0
-    for pid, g32 in groups32.items():
-        g64 = groups64.get(pid)
-        if g64 is None or len(g64) != len(g32):
-            continue
-        a, b = np.array(g32), np.array(g64)
-        if not np.allclose(a[:, 3:6], b[:, 3:6], rtol=0, atol=1e-3):
-            continue
-        agree += 1
-        scale = max(1.0, np.abs(b[:, 6]).max())
-        assert np.abs(a[:, 6] - b[:, 6]).max() <= 1e-5 * scale
-        assert np.abs(a[:, 3:6] - b[:, 3:6]).max() <= 1e-5
-    assert agree >= 0.9 * len(groups32)
+    A, B = sc.meshes
+    check_against_fp64(oracle, dev, golden[f"{key}_contacts_f64"], golden[f"{key}_xyzA"], A, golden[f"{key}_xyzB"],
+                       B, ref_pairs)
+
+
+def check_against_fp64(oracle, dev_rows, ref64_rows, xa, A, xb, B, pairs):
+    """Device FP32 contacts vs the FP64 oracle on the pairs whose discrete
+    decisions (overlap, chosen faces, set of generated contact candidates)
+    agree between FP32 and FP64.  Edge/face-plane crossing candidates lie on
+    their own plane, so the reference's inside test decides them by rounding
+    and the two precisions often keep different candidate sets; where they
+    keep the same set, depth and normal must agree within 1e-5 relative to
+    max(|depth|, one lattice cell)."""
+    _, rec32 = oracle.contacts(xa, A.tets, A.surf, xb, B.tets, B.surf, pairs, "f")
+    _, rec64 = oracle.contacts(xa, A.tets, A.surf, xb, B.tets, B.surf, pairs, "d")
+    same = ((rec32["face_a"] == rec64["face_a"]) & (rec32["face_b"] == rec64["face_b"])
+            & (rec32["overlap"] == rec64["overlap"]) & (rec32["cand_mask"] == rec64["cand_mask"]))
+    g32, g64 = {}, {}
+    for row in dev_rows:
+        g32.setdefault(int(row[7]), []).append(row)
+    for row in ref64_rows:
+        g64.setdefault(int(row[7]), []).append(row)
+    with_contacts = [p for p in g32]
+    agree = [p for p in with_contacts if same[p] and p in g64]
+    for p in agree:
+        a, b = np.array(g32[p], np.float64), np.array(g64[p])
+        scale = max(1.0, abs(b[0, 6]))
+        assert abs(a[0, 6] - b[0, 6]) <= 1e-5 * scale
+        assert np.abs(a[0, 3:6] - b[0, 3:6]).max() <= 1e-5
+    # Every contact-producing pair: the FP64 depth and normal evaluated with
+    # the FP32 run's discrete decisions (face, extreme candidates) frozen.
+    ta, tb = A.tets[pairs[:, 0]], B.tets[pairs[:, 1]]
+    for p in with_contacts:
+        a12 = xa[ta[p]].astype(np.float64).ravel()
+        b12 = xb[tb[p]].astype(np.float64).ravel()
+        d64, n64 = oracle.frozen_depth(a12, b12, rec32[p])
+        row = np.array(g32[p][0], np.float64)
+        assert abs(row[6] - d64) <= 1e-5 * max(1.0, abs(d64)), (p, row[6], d64)
+        assert np.abs(row[3:6] - n64).max() <= 1e-5, (p, row[3:6], n64)
+    return len(agree), len(with_contacts)
 
 
 @pytest.mark.parametrize("K", [6, 14, 26])
