@@ -594,8 +594,10 @@ static int resolve_opts(const kdop_scene* s, const kdop_traverse_opts* o, kdop::
   p.donate_min = o->donate_min > 0 ? o->donate_min : d.donate_min;
   p.timeout_ns = (long long)(o->timeout_ms > 0 ? o->timeout_ms : 5000) * 1000000ll;
   p.surface_filter = o->surface_filter ? 1 : 0;
+  p.load_group = o->load_group > 0 ? o->load_group : d.load_group;
   if (p.block_warps > 16 || (p.stack_cap & (p.stack_cap - 1)) || p.stack_cap < 64 || p.init_chunk > 32)
     return KDOP_ERR_INVALID;
+  if (p.load_group != 1 && p.load_group != 2 && p.load_group != 4) return KDOP_ERR_INVALID;
   if (kdop::traverse_smem_bytes(p.block_warps, p.stack_cap) > s->ctx->smem_optin) return KDOP_ERR_INVALID;
   return KDOP_OK;
 }
@@ -610,6 +612,7 @@ int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
   o->init_chunk = 1;
   o->donate_min = 64;
   o->timeout_ms = 5000;
+  o->load_group = 2;
   if (s) {
     kdop_scene_ext* x = ext(const_cast<kdop_scene*>(s));
     if (x->has_tuned) {
@@ -617,6 +620,7 @@ int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
       o->stack_cap = x->tuned.stack_cap;
       o->init_chunk = x->tuned.init_chunk;
       o->donate_min = x->tuned.donate_min;
+      o->load_group = x->tuned.load_group;
     }
   }
   return KDOP_OK;
@@ -886,10 +890,11 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   if (repeats < 1) repeats = 1;
   int rc = upload_pairs(s, n_pairs, pairs, memory);
   if (rc != KDOP_OK) return rc;
-  const int warps[] = {4, 8, 16};
+  const int warps[] = {8, 16};
   const int caps[] = {256, 512, 1024};
-  const int chunks[] = {1, 4};
+  const int chunks[] = {1};
   const int donate[] = {32, 96};
+  const int groups[] = {1, 2, 4};
   cudaEvent_t e0, e1;
   KDOP_CUDA(s->ctx, cudaEventCreate(&e0));
   KDOP_CUDA(s->ctx, cudaEventCreate(&e1));
@@ -899,8 +904,10 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   for (int w : warps)
     for (int c : caps)
       for (int ch : chunks)
-        for (int dm : donate) {
+        for (int dm : donate)
+          for (int lg : groups) {
           kdop::TravParams p;
+          p.load_group = lg;
           p.block_warps = w;
           p.stack_cap = c;
           p.init_chunk = ch;
@@ -935,6 +942,7 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
             bo.stack_cap = c;
             bo.init_chunk = ch;
             bo.donate_min = dm;
+            bo.load_group = lg;
           }
         }
   cudaEventDestroy(e0);

@@ -51,6 +51,7 @@ struct TravParams {
   int donate_min;
   long long timeout_ns;
   int surface_filter;
+  int load_group;
 };
 
 }  // namespace kdop

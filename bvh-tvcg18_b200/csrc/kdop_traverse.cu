@@ -63,14 +63,43 @@ __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volati
 
 // Overlap of the child pairs of one deque entry.  Side X is either a leaf
 // node (1 candidate: the node itself) or an internal node given by its first
-// child c (2 candidates: c, c + 1).
-template <int K>
+// child c (2 candidates: c, c + 1).  The records are fetched G float4 chunks
+// per round (all loads of a round in flight together); the next round is only
+// fetched while some child pair is still undecided.
+template <int K, int G>
 struct Expand {
   using L = NodeLayout<K>;
   uint32_t idxA[2], idxB[2];  // node indices of the candidates
   uint32_t stA[2], enA[2], stB[2], enB[2];
   int na, nb;
   unsigned sep;  // bit (2 i + k): child pair (i, k) separated (or absent)
+
+  __device__ __forceinline__ void chunk(int j, const float4& A0, const float4& A1, const float4& B0,
+                                        const float4& B1) {
+    if (2 * j < L::NS) {
+      // separated iff A.hi < B.lo || B.hi < A.lo
+      sep |= ((A0.y < B0.x) || (B0.y < A0.x)) ? 1u : 0u;
+      sep |= ((A0.y < B1.x) || (B1.y < A0.x)) ? 2u : 0u;
+      sep |= ((A1.y < B0.x) || (B0.y < A1.x)) ? 4u : 0u;
+      sep |= ((A1.y < B1.x) || (B1.y < A1.x)) ? 8u : 0u;
+    }
+    if (2 * j + 1 < L::NS) {
+      sep |= ((A0.w < B0.z) || (B0.w < A0.z)) ? 1u : 0u;
+      sep |= ((A0.w < B1.z) || (B1.w < A0.z)) ? 2u : 0u;
+      sep |= ((A1.w < B0.z) || (B0.w < A1.z)) ? 4u : 0u;
+      sep |= ((A1.w < B1.z) || (B1.w < A1.z)) ? 8u : 0u;
+    }
+    if (j == L::TOPO_CHUNK) {
+      stA[0] = __float_as_uint(L::TOPO_ZW ? A0.z : A0.x);
+      enA[0] = __float_as_uint(L::TOPO_ZW ? A0.w : A0.y);
+      stA[1] = __float_as_uint(L::TOPO_ZW ? A1.z : A1.x);
+      enA[1] = __float_as_uint(L::TOPO_ZW ? A1.w : A1.y);
+      stB[0] = __float_as_uint(L::TOPO_ZW ? B0.z : B0.x);
+      enB[0] = __float_as_uint(L::TOPO_ZW ? B0.w : B0.y);
+      stB[1] = __float_as_uint(L::TOPO_ZW ? B1.z : B1.x);
+      enB[1] = __float_as_uint(L::TOPO_ZW ? B1.w : B1.y);
+    }
+  }
 
   __device__ __forceinline__ void run(const float4* __restrict__ nodes, uint32_t ea, uint32_t eb) {
     na = (ea & LEAF_BIT) ? 1 : 2;
@@ -87,42 +116,29 @@ struct Expand {
     const float4* pb = nodes + (int64_t)b0 * L::NW;
     stA[0] = stA[1] = enA[0] = enA[1] = stB[0] = stB[1] = enB[0] = enB[1] = 0;
 #pragma unroll
-    for (int j = 0; j < L::NW; ++j) {
+    for (int j0 = 0; j0 < L::NW; j0 += G) {
       if (sep == 0xF) break;
-      float4 A0 = __ldg(pa + j);
-      float4 B0 = __ldg(pb + j);
-      float4 A1 = A0, B1 = B0;
-      if (na == 2) A1 = __ldg(pa + L::NW + j);
-      if (nb == 2) B1 = __ldg(pb + L::NW + j);
-      if (2 * j < L::NS) {
-        // separated iff A.hi < B.lo || B.hi < A.lo
-        sep |= ((A0.y < B0.x) || (B0.y < A0.x)) ? 1u : 0u;
-        sep |= ((A0.y < B1.x) || (B1.y < A0.x)) ? 2u : 0u;
-        sep |= ((A1.y < B0.x) || (B0.y < A1.x)) ? 4u : 0u;
-        sep |= ((A1.y < B1.x) || (B1.y < A1.x)) ? 8u : 0u;
+      float4 A0[G], A1[G], B0[G], B1[G];
+#pragma unroll
+      for (int g = 0; g < G; ++g) {
+        if (j0 + g < L::NW) {
+          A0[g] = __ldg(pa + j0 + g);
+          B0[g] = __ldg(pb + j0 + g);
+          A1[g] = A0[g];
+          B1[g] = B0[g];
+          if (na == 2) A1[g] = __ldg(pa + L::NW + j0 + g);
+          if (nb == 2) B1[g] = __ldg(pb + L::NW + j0 + g);
+        }
       }
-      if (2 * j + 1 < L::NS) {
-        sep |= ((A0.w < B0.z) || (B0.w < A0.z)) ? 1u : 0u;
-        sep |= ((A0.w < B1.z) || (B1.w < A0.z)) ? 2u : 0u;
-        sep |= ((A1.w < B0.z) || (B0.w < A1.z)) ? 4u : 0u;
-        sep |= ((A1.w < B1.z) || (B1.w < A1.z)) ? 8u : 0u;
-      }
-      if (j == L::TOPO_CHUNK) {
-        stA[0] = __float_as_uint(L::TOPO_ZW ? A0.z : A0.x);
-        enA[0] = __float_as_uint(L::TOPO_ZW ? A0.w : A0.y);
-        stA[1] = __float_as_uint(L::TOPO_ZW ? A1.z : A1.x);
-        enA[1] = __float_as_uint(L::TOPO_ZW ? A1.w : A1.y);
-        stB[0] = __float_as_uint(L::TOPO_ZW ? B0.z : B0.x);
-        enB[0] = __float_as_uint(L::TOPO_ZW ? B0.w : B0.y);
-        stB[1] = __float_as_uint(L::TOPO_ZW ? B1.z : B1.x);
-        enB[1] = __float_as_uint(L::TOPO_ZW ? B1.w : B1.y);
-      }
+#pragma unroll
+      for (int g = 0; g < G; ++g)
+        if (j0 + g < L::NW) chunk(j0 + g, A0[g], A1[g], B0[g], B1[g]);
     }
   }
 };
 
-template <int K>
-__global__ void __launch_bounds__(512) traverse_kernel(TravArgs a) {
+template <int K, int G>
+__global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
   extern __shared__ uint32_t smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
@@ -149,9 +165,18 @@ __global__ void __launch_bounds__(512) traverse_kernel(TravArgs a) {
     uint32_t pushA[4], pushB[4], emitA[4], emitB[4];
     uint32_t pid = 0;
 
+    // queue counters for the donation check, read early so that their
+    // latency overlaps the node loads of this step
+    unsigned q_h = 0, q_t = 0;
+    if (lane == 0 && top - bot >= a.donate_min) {
+      q_h = ld_volatile(&ctl->q_head);
+      q_t = ld_volatile(&ctl->q_tail);
+    }
+
     if (top == bot) {
+      // Work handed to the queue was counted before it was published, so the
+      // release needs no fence.
       if (release) {
-        __threadfence();
         if (lane == 0) atomicSub(&ctl->work, release);
         release = 0;
       }
@@ -171,7 +196,7 @@ __global__ void __launch_bounds__(512) traverse_kernel(TravArgs a) {
             uint2 mp = a.pairs[pid];
             uint32_t ra = a.root[mp.x], rb = a.root[mp.y];
             if (ra != NO_NODE && rb != NO_NODE) {
-              Expand<K> ex;
+              Expand<K, G> ex;
               ex.run(a.nodes, ra | LEAF_BIT, rb | LEAF_BIT);
               my_tests += 1;
               if (!(ex.sep & 1u)) {
@@ -246,7 +271,7 @@ __global__ void __launch_bounds__(512) traverse_kernel(TravArgs a) {
         int at = (top + lane) & MASK;
         uint32_t ea = sA[at], eb = sB[at];
         pid = sP[at];
-        Expand<K> ex;
+        Expand<K, G> ex;
         ex.run(a.nodes, ea, eb);
         my_tests += (unsigned long long)(ex.na * ex.nb);
 #pragma unroll
@@ -350,10 +375,7 @@ __global__ void __launch_bounds__(512) traverse_kernel(TravArgs a) {
     // ---- donation: give the oldest entries to waiting warps ----
     if (depth >= a.donate_min) {
       int waiting = 0;
-      if (lane == 0) {
-        unsigned h = ld_volatile(&ctl->q_head), t = ld_volatile(&ctl->q_tail);
-        waiting = (h > t) ? (int)min(h - t, 32u) : 0;
-      }
+      if (lane == 0) waiting = (q_h > q_t) ? (int)min(q_h - q_t, 32u) : 0;
       waiting = __shfl_sync(0xffffffffu, waiting, 0);
       int d = min(waiting, depth / 2);
       if (d > 0) {
@@ -417,7 +439,12 @@ size_t traverse_smem_bytes(int block_warps, int stack_cap) {
 
 template <int K>
 static cudaError_t prepare_k(size_t smem) {
-  return cudaFuncSetAttribute(traverse_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(traverse_kernel<K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(traverse_kernel<K, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(traverse_kernel<K, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return e;
 }
 
 cudaError_t traverse_prepare(int K, size_t smem) {
@@ -433,7 +460,7 @@ cudaError_t traverse_prepare(int K, size_t smem) {
   return cudaErrorInvalidValue;
 }
 
-template <int K>
+template <int K, int G>
 static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p,
                                  int plain) {
   cudaStream_t st = s->ctx->stream;
@@ -442,7 +469,7 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const uint2* pa
   cudaError_t e = prepare_k<K>(smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_kernel<K>, threads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_kernel<K, G>, threads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   unsigned grid = (unsigned)(per_sm * s->ctx->sm_count);
@@ -466,12 +493,12 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const uint2* pa
   a.timeout_ns = p.timeout_ns;
   if (!plain) {
     trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, (unsigned)n_pairs, 0u, 1);
-    traverse_kernel<K><<<grid, threads, smem, st>>>(a);
+    traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
     s->ctx->launches += 2;
   } else {
     for (int64_t i = 0; i < n_pairs; ++i) {
       trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, 1u, (unsigned)i, i == 0 ? 1 : 0);
-      traverse_kernel<K><<<grid, threads, smem, st>>>(a);
+      traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
       s->ctx->launches += 2;
     }
     if (n_pairs == 0) {
@@ -482,15 +509,25 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const uint2* pa
   return cudaGetLastError();
 }
 
+template <int K>
+static cudaError_t traverse_group(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p,
+                                  int plain) {
+  switch (p.load_group) {
+    case 1: return traverse_impl<K, 1>(s, n_pairs, pairs, p, plain);
+    case 4: return traverse_impl<K, 4>(s, n_pairs, pairs, p, plain);
+    default: return traverse_impl<K, 2>(s, n_pairs, pairs, p, plain);
+  }
+}
+
 cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int plain) {
   switch (s->K) {
-    case 6: return traverse_impl<6>(s, n_pairs, pairs, p, plain);
-    case 8: return traverse_impl<8>(s, n_pairs, pairs, p, plain);
-    case 12: return traverse_impl<12>(s, n_pairs, pairs, p, plain);
-    case 14: return traverse_impl<14>(s, n_pairs, pairs, p, plain);
-    case 18: return traverse_impl<18>(s, n_pairs, pairs, p, plain);
-    case 20: return traverse_impl<20>(s, n_pairs, pairs, p, plain);
-    case 26: return traverse_impl<26>(s, n_pairs, pairs, p, plain);
+    case 6: return traverse_group<6>(s, n_pairs, pairs, p, plain);
+    case 8: return traverse_group<8>(s, n_pairs, pairs, p, plain);
+    case 12: return traverse_group<12>(s, n_pairs, pairs, p, plain);
+    case 14: return traverse_group<14>(s, n_pairs, pairs, p, plain);
+    case 18: return traverse_group<18>(s, n_pairs, pairs, p, plain);
+    case 20: return traverse_group<20>(s, n_pairs, pairs, p, plain);
+    case 26: return traverse_group<26>(s, n_pairs, pairs, p, plain);
   }
   return cudaErrorInvalidValue;
 }

@@ -149,7 +149,7 @@ typedef struct {
   int32_t init_chunk;     /* root pairs taken per queue claim (0: default) */
   int32_t donate_min;     /* stack size from which a warp gives work to idle warps (0: default) */
   int32_t timeout_ms;     /* bound of every device-side wait (0: 5000) */
-  int32_t reserved;
+  int32_t load_group;     /* float4 chunks of a node record fetched per round: 1, 2 or 4 (0: default) */
 } kdop_traverse_opts;
 
 /* Fills opts with the defaults (or the autotuned choice cached for this scene). */
