@@ -582,7 +582,9 @@ int kdop_read_vertices(kdop_scene* s, float* xyz, int64_t cap) {
   return KDOP_OK;
 }
 
-static int resolve_opts(const kdop_scene* s, const kdop_traverse_opts* o, kdop::TravParams& p, int& mode) {
+}  // extern "C"
+
+int kdop_resolve_traverse_opts(const kdop_scene* s, const kdop_traverse_opts* o, kdop::TravParams& p, int& mode) {
   kdop_traverse_opts d;
   kdop_traverse_opts_default(s, &d);
   if (!o) o = &d;
@@ -601,6 +603,8 @@ static int resolve_opts(const kdop_scene* s, const kdop_traverse_opts* o, kdop::
   if (kdop::traverse_smem_bytes(p.block_warps, p.stack_cap) > s->ctx->smem_optin) return KDOP_ERR_INVALID;
   return KDOP_OK;
 }
+
+extern "C" {
 
 int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
   if (!o) return KDOP_ERR_INVALID;
@@ -658,7 +662,7 @@ int kdop_traverse(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   cudaSetDevice(s->ctx->device);
   kdop::TravParams p;
   int mode = 0;
-  if (resolve_opts(s, opts, p, mode) != KDOP_OK) return fail(s->ctx, KDOP_ERR_INVALID, "bad traversal options");
+  if (kdop_resolve_traverse_opts(s, opts, p, mode) != KDOP_OK) return fail(s->ctx, KDOP_ERR_INVALID, "bad traversal options");
   int rc = upload_pairs(s, n_pairs, pairs, memory);
   if (rc != KDOP_OK) return rc;
   KDOP_CUDA(s->ctx, kdop::launch_traverse(s, n_pairs, s->pairs, p, mode == KDOP_TRAVERSE_PLAIN));
@@ -835,7 +839,7 @@ int kdop_graph_capture(kdop_scene* s, int refit_mode, int64_t n_pairs, const uin
   cudaSetDevice(s->ctx->device);
   kdop::TravParams p;
   int mode = 0;
-  if (resolve_opts(s, opts, p, mode) != KDOP_OK) return fail(s->ctx, KDOP_ERR_INVALID, "bad traversal options");
+  if (kdop_resolve_traverse_opts(s, opts, p, mode) != KDOP_OK) return fail(s->ctx, KDOP_ERR_INVALID, "bad traversal options");
   kdop_graph_release(s);
   int rc = upload_pairs(s, n_pairs, pairs, memory);
   if (rc != KDOP_OK) return rc;

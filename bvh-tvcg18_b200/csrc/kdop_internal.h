@@ -149,6 +149,13 @@ cudaError_t launch_adjoint(kdop_scene* s, const float* dd, const float* dn, floa
 cudaError_t launch_motion(kdop_scene* s);
 cudaError_t launch_world(kdop_scene* s, int mode, float4* out);
 int traverse_block_threads(int block_warps);
+
+}  // namespace kdop
+
+// Defaults + validation of traversal options (kdop_capi.cpp).
+int kdop_resolve_traverse_opts(const kdop_scene* s, const kdop_traverse_opts* o, kdop::TravParams& p, int& mode);
+
+namespace kdop {
 size_t traverse_smem_bytes(int block_warps, int stack_cap);
 cudaError_t traverse_prepare(int K, size_t smem);
 

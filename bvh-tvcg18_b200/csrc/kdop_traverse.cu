@@ -51,6 +51,19 @@ struct TravArgs {
   int donate_min;
   int surface_filter;
   long long timeout_ns;
+  unsigned n_meshes;
+};
+
+// Device buffers one traversal works in: pairs (input), candidates (output),
+// work queue and control block (scratch).
+struct TravBuffers {
+  const uint2* pairs;
+  uint32_t* cand;  // 3 * cand_cap: A tets | B tets | pair ids
+  int64_t cand_cap;
+  uint4* q_items;
+  uint32_t* q_tags;
+  int64_t q_cap;
+  TravCtl* ctl;
 };
 
 __device__ __forceinline__ unsigned long long global_ns() {
@@ -194,7 +207,13 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
             // test of the root pair (:42), both counted as the reference does.
             pid = pair_base + base + lane;
             uint2 mp = a.pairs[pid];
-            uint32_t ra = a.root[mp.x], rb = a.root[mp.y];
+            uint32_t ra = NO_NODE, rb = NO_NODE;
+            if (mp.x < a.n_meshes && mp.y < a.n_meshes) {
+              ra = a.root[mp.x];
+              rb = a.root[mp.y];
+            } else {
+              atomicOr(&ctl->error, DEV_ERR_BAD_INDEX);
+            }
             if (ra != NO_NODE && rb != NO_NODE) {
               Expand<K, G> ex;
               ex.run(a.nodes, ra | LEAF_BIT, rb | LEAF_BIT);
@@ -461,7 +480,7 @@ cudaError_t traverse_prepare(int K, size_t smem) {
 }
 
 template <int K, int G>
-static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p,
+static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffers& b, const TravParams& p,
                                  int plain) {
   cudaStream_t st = s->ctx->stream;
   int threads = traverse_block_threads(p.block_warps);
@@ -477,32 +496,33 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const uint2* pa
   a.nodes = s->nodes;
   a.surf = s->surf;
   a.root = s->root_dev;
-  a.pairs = pairs;
-  a.candA = s->cand;
-  a.candB = s->cand + s->cand_cap;
-  a.candP = s->cand + 2 * s->cand_cap;
-  a.cand_cap = (unsigned)s->cand_cap;
-  a.q_items = s->q_items;
-  a.q_tags = s->q_tags;
-  a.q_cap = (unsigned)s->queue_cap;
-  a.ctl = s->ctl;
+  a.pairs = b.pairs;
+  a.candA = b.cand;
+  a.candB = b.cand + b.cand_cap;
+  a.candP = b.cand + 2 * b.cand_cap;
+  a.cand_cap = (unsigned)b.cand_cap;
+  a.q_items = b.q_items;
+  a.q_tags = b.q_tags;
+  a.q_cap = (unsigned)b.q_cap;
+  a.ctl = b.ctl;
+  a.n_meshes = (unsigned)s->n_meshes;
   a.stack_cap = p.stack_cap;
   a.init_chunk = p.init_chunk;
   a.donate_min = p.donate_min;
   a.surface_filter = p.surface_filter;
   a.timeout_ns = p.timeout_ns;
   if (!plain) {
-    trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, (unsigned)n_pairs, 0u, 1);
+    trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)n_pairs, 0u, 1);
     traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
     s->ctx->launches += 2;
   } else {
     for (int64_t i = 0; i < n_pairs; ++i) {
-      trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, 1u, (unsigned)i, i == 0 ? 1 : 0);
+      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 1u, (unsigned)i, i == 0 ? 1 : 0);
       traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
       s->ctx->launches += 2;
     }
     if (n_pairs == 0) {
-      trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, 0u, 0u, 1);
+      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 0u, 0u, 1);
       s->ctx->launches += 1;
     }
   }
@@ -510,26 +530,40 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const uint2* pa
 }
 
 template <int K>
-static cudaError_t traverse_group(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p,
+static cudaError_t traverse_group(kdop_scene* s, int64_t n_pairs, const TravBuffers& b, const TravParams& p,
                                   int plain) {
   switch (p.load_group) {
-    case 1: return traverse_impl<K, 1>(s, n_pairs, pairs, p, plain);
-    case 4: return traverse_impl<K, 4>(s, n_pairs, pairs, p, plain);
-    default: return traverse_impl<K, 2>(s, n_pairs, pairs, p, plain);
+    case 1: return traverse_impl<K, 1>(s, n_pairs, b, p, plain);
+    case 4: return traverse_impl<K, 4>(s, n_pairs, b, p, plain);
+    default: return traverse_impl<K, 2>(s, n_pairs, b, p, plain);
   }
 }
 
-cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int plain) {
+static cudaError_t traverse_buffers(kdop_scene* s, int64_t n_pairs, const TravBuffers& b, const TravParams& p,
+                                    int plain) {
   switch (s->K) {
-    case 6: return traverse_group<6>(s, n_pairs, pairs, p, plain);
-    case 8: return traverse_group<8>(s, n_pairs, pairs, p, plain);
-    case 12: return traverse_group<12>(s, n_pairs, pairs, p, plain);
-    case 14: return traverse_group<14>(s, n_pairs, pairs, p, plain);
-    case 18: return traverse_group<18>(s, n_pairs, pairs, p, plain);
-    case 20: return traverse_group<20>(s, n_pairs, pairs, p, plain);
-    case 26: return traverse_group<26>(s, n_pairs, pairs, p, plain);
+    case 6: return traverse_group<6>(s, n_pairs, b, p, plain);
+    case 8: return traverse_group<8>(s, n_pairs, b, p, plain);
+    case 12: return traverse_group<12>(s, n_pairs, b, p, plain);
+    case 14: return traverse_group<14>(s, n_pairs, b, p, plain);
+    case 18: return traverse_group<18>(s, n_pairs, b, p, plain);
+    case 20: return traverse_group<20>(s, n_pairs, b, p, plain);
+    case 26: return traverse_group<26>(s, n_pairs, b, p, plain);
   }
   return cudaErrorInvalidValue;
 }
 
+cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int plain) {
+  TravBuffers b;
+  b.pairs = pairs;
+  b.cand = s->cand;
+  b.cand_cap = s->cand_cap;
+  b.q_items = s->q_items;
+  b.q_tags = s->q_tags;
+  b.q_cap = s->queue_cap;
+  b.ctl = s->ctl;
+  return traverse_buffers(s, n_pairs, b, p, plain);
+}
+
 }  // namespace kdop
+
