@@ -29,6 +29,8 @@
 //   * termination: a global count of outstanding work units reaches zero;
 //     every wait is bounded by a time limit after which the kernel records
 //     DEV_ERR_TIMEOUT and returns (no unbounded spin).
+#include <mutex>
+
 #include "kdop_device.cuh"
 
 namespace kdop {
@@ -567,3 +569,90 @@ cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, 
 
 }  // namespace kdop
 
+// ---- traversal that allocates no device memory -------------------------------
+// Its scratch -- the traversal's control block and work queue -- lives in this
+// file-scope device array instead of the scene's allocated buffers.  Every GPU
+// that loads the library holds the array until the process exits.
+namespace kdop {
+namespace {
+
+constexpr int64_t kStaticQueueEntries = 65536;
+constexpr size_t kStaticCtlBytes = 256;
+constexpr size_t kStaticTagBytes = (size_t)kStaticQueueEntries * sizeof(uint32_t);
+constexpr size_t kStaticScratchBytes = kStaticCtlBytes + kStaticTagBytes + (size_t)kStaticQueueEntries * sizeof(uint4);
+static_assert(sizeof(TravCtl) <= kStaticCtlBytes, "control block does not fit");
+
+__device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch per device, found once per device with
+// that device current.  In host code the array's name only stands in for the
+// symbol; it is not a device address.
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+void* g_static_addr[kMaxDevices] = {nullptr};
+
+cudaError_t static_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess) return e;
+    g_static_addr[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_static_addr[device]);
+  return cudaSuccess;
+}
+
+__global__ void static_counters_kernel(const TravCtl* c, unsigned long long* out) {
+  if (threadIdx.x != 0) return;
+  out[0] = c->n_cand;
+  out[1] = c->tests;
+  out[2] = c->leaf_overlaps;
+  out[3] = c->error;
+}
+
+}  // namespace
+}  // namespace kdop
+
+extern "C" int kdop_traverse_noalloc(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, uint32_t* candidates,
+                                     int64_t cap, unsigned long long* counters, const kdop_traverse_opts* opts) {
+  using namespace kdop;
+  if (!s || n_pairs < 0 || (n_pairs > 0 && !pairs) || !candidates || cap <= 0 || !counters) return KDOP_ERR_INVALID;
+  if (cap > (int64_t)0xFFFFFFF0ll || n_pairs >= (int64_t)0x7FFFFFFF) return KDOP_ERR_CAPACITY;
+  TravParams p;
+  int mode = 0;
+  if (kdop_resolve_traverse_opts(s, opts, p, mode) != KDOP_OK) return KDOP_ERR_INVALID;
+  if (cudaSetDevice(s->ctx->device) != cudaSuccess) return KDOP_ERR_CUDA;
+  unsigned char* base = nullptr;
+  if (static_scratch(s->ctx->device, &base) != cudaSuccess) {
+    cudaGetLastError();
+    return KDOP_ERR_CUDA;
+  }
+  TravBuffers b;
+  b.pairs = reinterpret_cast<const uint2*>(pairs);
+  b.cand = candidates;
+  b.cand_cap = cap;
+  b.ctl = reinterpret_cast<TravCtl*>(base);
+  b.q_tags = reinterpret_cast<uint32_t*>(base + kStaticCtlBytes);
+  b.q_items = reinterpret_cast<uint4*>(base + kStaticCtlBytes + kStaticTagBytes);
+  b.q_cap = kStaticQueueEntries;
+  cudaStream_t st = s->ctx->stream;
+  // the array keeps the previous call's contents: the control block and the
+  // queue tags must start at zero
+  if (cudaMemsetAsync(base, 0, kStaticCtlBytes + kStaticTagBytes, st) != cudaSuccess) {
+    cudaGetLastError();
+    return KDOP_ERR_CUDA;
+  }
+  cudaError_t e = traverse_buffers(s, n_pairs, b, p, mode == KDOP_TRAVERSE_PLAIN);
+  if (e == cudaSuccess) {
+    static_counters_kernel<<<1, 32, 0, st>>>(b.ctl, counters);
+    s->ctx->launches += 1;
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return KDOP_ERR_CUDA;
+  }
+  return KDOP_OK;
+}

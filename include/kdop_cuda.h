@@ -186,6 +186,31 @@ int kdop_reserve(kdop_scene* scene, int64_t candidates, int64_t contacts, int64_
 /* Sets the three capacities exactly (0 = keep), e.g. to bound device memory. */
 int kdop_set_capacity(kdop_scene* scene, int64_t candidates, int64_t contacts, int64_t queue);
 
+/* Tandem traversal that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc while they
+ * run -- code recording a caller-owned stream into a CUDA graph (device
+ * allocation is not allowed during capture), simulators that keep a fixed
+ * device-memory budget or arena for the whole run, and real-time loops that
+ * must not risk an allocation failure mid-step.
+ *
+ * The caller passes device memory only: pairs (n_pairs * 2 mesh indices),
+ * candidates (3 * cap uint32: tets of A | tets of B | pair indices; tet
+ * indices are scene-global, i.e. mesh m's tets start at the tet count of the
+ * meshes before m) and counters (4 uint64: candidates found -- more than cap
+ * means the rows were cut --, node-pair tests, overlapping leaf pairs, device
+ * error bits).  The traversal's control block and work queue live in a static
+ * device array of 1.25 MiB per GPU (a queue of 65,536 entries) that every GPU
+ * loading the library keeps until the process exits; a run that needs more
+ * queue entries sets error bit 2 in counters[3] and is incomplete (use
+ * kdop_traverse then).  cap above 2^32 - 16 or n_pairs of 2^31 - 1 or more
+ * are rejected with KDOP_ERR_CAPACITY.  Calls share the array, so calls that
+ * overlap on the GPU (other streams, other threads) race; each call clears the
+ * parts that must start at zero.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress, once per device): make that
+ * first call before any stream capture.  Asynchronous on the scene's stream. */
+int kdop_traverse_noalloc(kdop_scene* scene, int64_t n_pairs, const uint32_t* pairs, uint32_t* candidates,
+                          int64_t cap, unsigned long long* counters, const kdop_traverse_opts* opts);
+
 /* Candidate rows (pair index, mesh-local tet of A, mesh-local tet of B) in the
  * device's emission order; sort them for a canonical order. Synchronises. */
 int kdop_read_candidates(kdop_scene* scene, uint32_t* rows, int64_t cap_rows, int64_t* n_rows);
