@@ -343,70 +343,78 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK_C) contacts_kernel(Contac
 // a + (b - a) t, t = |sA| / (|sA| + |sB|), s = m_p . (x - F0) for the face
 // plane p of the other tet.  In exact arithmetic the three corner cross
 // products of make_unscaled_plane coincide and every corner lies on the
-// plane, so the first corner stands for the chosen one.
-struct G3 {
-  float x, y, z;
+// plane, so the first corner stands for the chosen one.  The inputs and the
+// gradient are float; the chain rule runs in double, because near-parallel
+// edge/plane crossings (dA + dB small) amplify rounding by orders of
+// magnitude.
+struct d3 {
+  double x, y, z;
 };
-__device__ __forceinline__ f3 face_m(const f3* T, int f, f3& F0) {
+__device__ __forceinline__ d3 dmk(double x, double y, double z) { return d3{x, y, z}; }
+__device__ __forceinline__ d3 dof(f3 v) { return d3{(double)v.x, (double)v.y, (double)v.z}; }
+__device__ __forceinline__ d3 dsub(d3 a, d3 b) { return dmk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ d3 dadd(d3 a, d3 b) { return dmk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ d3 dscl(d3 a, double s) { return dmk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ double ddot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ d3 dcross(d3 l, d3 r) {
+  return dmk(l.y * r.z - l.z * r.y, l.z * r.x - l.x * r.z, l.x * r.y - l.y * r.x);
+}
+__device__ __forceinline__ void dacc(d3* g, int i, d3 v) { g[i] = dadd(g[i], v); }
+
+__device__ __forceinline__ d3 face_m(const d3* T, int f, d3& F0) {
   F0 = T[c_face[f][0]];
-  return cross3(sub3(T[c_face[f][1]], F0), sub3(T[c_face[f][2]], F0));
+  return dcross(dsub(T[c_face[f][1]], F0), dsub(T[c_face[f][2]], F0));
 }
-__device__ __forceinline__ void acc(f3* g, int i, f3 v) { g[i] = mk3(g[i].x + v.x, g[i].y + v.y, g[i].z + v.z); }
-__device__ __forceinline__ f3 fcross(f3 l, f3 r) {
-  return mk3(l.y * r.z - l.z * r.y, l.z * r.x - l.x * r.z, l.x * r.y - l.y * r.x);
-}
-__device__ __forceinline__ float fdot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-__device__ __forceinline__ f3 fs(f3 a, float s) { return mk3(a.x * s, a.y * s, a.z * s); }
-__device__ __forceinline__ f3 fsub3(f3 a, f3 b) { return mk3(a.x - b.x, a.y - b.y, a.z - b.z); }
-__device__ __forceinline__ f3 fadd3(f3 a, f3 b) { return mk3(a.x + b.x, a.y + b.y, a.z + b.z); }
 
-__device__ void face_m_adj(const f3* T, int f, f3 gm, f3* gT) {
+// adjoint of m = (P1 - P0) x (P2 - P0) for face f of T into gT
+__device__ void face_m_adj(const d3* T, int f, d3 gm, d3* gT) {
   int i0 = c_face[f][0], i1 = c_face[f][1], i2 = c_face[f][2];
-  f3 u = fsub3(T[i1], T[i0]), w = fsub3(T[i2], T[i0]);
-  f3 gu = fcross(w, gm), gw = fcross(gm, u);
-  acc(gT, i1, gu);
-  acc(gT, i2, gw);
-  acc(gT, i0, mk3(-(gu.x + gw.x), -(gu.y + gw.y), -(gu.z + gw.z)));
+  d3 u = dsub(T[i1], T[i0]), w = dsub(T[i2], T[i0]);
+  d3 gu = dcross(w, gm), gw = dcross(gm, u);
+  dacc(gT, i1, gu);
+  dacc(gT, i2, gw);
+  dacc(gT, i0, dscl(dadd(gu, gw), -1.0));
 }
 
-__device__ f3 cand_point(int c, const f3* A, const f3* B) {
+__device__ d3 cand_point(int c, const d3* A, const d3* B) {
   if (c < 8) return (c & 1) ? A[c >> 1] : B[c >> 1];
   int e = (c - 8) >> 3, p = ((c - 8) >> 1) & 3;
-  const f3* E = (c & 1) ? A : B;
-  const f3* T = (c & 1) ? B : A;
-  f3 a = E[c_edge[e][0]], b = E[c_edge[e][1]], F0;
-  f3 m = face_m(T, p, F0);
-  float dA = fabsf(fdot(m, fsub3(a, F0))), dB = fabsf(fdot(m, fsub3(b, F0)));
-  float t = dA / (dA + dB);
-  return fadd3(a, fs(fsub3(b, a), t));
+  const d3* E = (c & 1) ? A : B;
+  const d3* T = (c & 1) ? B : A;
+  d3 a = E[c_edge[e][0]], b = E[c_edge[e][1]], F0;
+  d3 m = face_m(T, p, F0);
+  double dA = fabs(ddot(m, dsub(a, F0))), dB = fabs(ddot(m, dsub(b, F0)));
+  double t = dA / (dA + dB);
+  return dadd(a, dscl(dsub(b, a), t));
 }
 
-__device__ void cand_adj(int c, const f3* A, const f3* B, f3 gq, f3* gA, f3* gB) {
+__device__ void cand_adj(int c, const d3* A, const d3* B, d3 gq, d3* gA, d3* gB) {
   if (c < 8) {
-    acc((c & 1) ? gA : gB, c >> 1, gq);
+    dacc((c & 1) ? gA : gB, c >> 1, gq);
     return;
   }
   int e = (c - 8) >> 3, p = ((c - 8) >> 1) & 3;
-  const f3* E = (c & 1) ? A : B;
-  const f3* T = (c & 1) ? B : A;
-  f3* gE = (c & 1) ? gA : gB;
-  f3* gT = (c & 1) ? gB : gA;
+  const d3* E = (c & 1) ? A : B;
+  const d3* T = (c & 1) ? B : A;
+  d3* gE = (c & 1) ? gA : gB;
+  d3* gT = (c & 1) ? gB : gA;
   int ia = c_edge[e][0], ib = c_edge[e][1];
-  f3 a = E[ia], b = E[ib], F0;
-  f3 m = face_m(T, p, F0);
-  float sA = fdot(m, fsub3(a, F0)), sB = fdot(m, fsub3(b, F0));
-  float sgA = sA < 0.f ? -1.f : 1.f, sgB = sB < 0.f ? -1.f : 1.f;
-  float dA = fabsf(sA), dB = fabsf(sB), S = dA + dB;
-  float t = dA / S;
-  acc(gE, ia, fs(gq, 1.f - t));
-  acc(gE, ib, fs(gq, t));
-  float gt = fdot(gq, fsub3(b, a));
-  float gdA = gt * dB / (S * S), gdB = -gt * dA / (S * S);
-  acc(gE, ia, fs(m, sgA * gdA));
-  acc(gE, ib, fs(m, sgB * gdB));
-  f3 gF = fadd3(fs(m, sgA * gdA), fs(m, sgB * gdB));
-  acc(gT, c_face[p][0], mk3(-gF.x, -gF.y, -gF.z));
-  f3 gm = fadd3(fs(fsub3(a, F0), sgA * gdA), fs(fsub3(b, F0), sgB * gdB));
+  d3 a = E[ia], b = E[ib], F0;
+  d3 m = face_m(T, p, F0);
+  double sA = ddot(m, dsub(a, F0)), sB = ddot(m, dsub(b, F0));
+  double sgA = sA < 0.0 ? -1.0 : 1.0, sgB = sB < 0.0 ? -1.0 : 1.0;
+  double dA = fabs(sA), dB = fabs(sB), S = dA + dB;
+  double t = dA / S;
+  // q = a + (b - a) t
+  dacc(gE, ia, dscl(gq, 1.0 - t));
+  dacc(gE, ib, dscl(gq, t));
+  double gt = ddot(gq, dsub(b, a));
+  double gdA = gt * dB / (S * S), gdB = -gt * dA / (S * S);
+  // dA = sgA m.(a - F0), dB = sgB m.(b - F0)
+  dacc(gE, ia, dscl(m, sgA * gdA));
+  dacc(gE, ib, dscl(m, sgB * gdB));
+  dacc(gT, c_face[p][0], dscl(dadd(dscl(m, sgA * gdA), dscl(m, sgB * gdB)), -1.0));
+  d3 gm = dadd(dscl(dsub(a, F0), sgA * gdA), dscl(dsub(b, F0), sgB * gdB));
   face_m_adj(T, p, gm, gT);
 }
 
@@ -429,40 +437,41 @@ __global__ void __launch_bounds__(128) adjoint_kernel(AdjointArgs a) {
   for (unsigned ci = blockIdx.x * blockDim.x + threadIdx.x; ci < n_cand; ci += gridDim.x * blockDim.x) {
     int4 r = a.rec[ci];
     if (r.z <= 0 || r.x < 0) continue;
-    float gd = 0.f;
-    f3 gn = mk3(0.f, 0.f, 0.f);
+    double gd = 0.0;
+    d3 gn = dmk(0.0, 0.0, 0.0);
     for (int k = 0; k < r.z; ++k) {
       unsigned row = (unsigned)r.w + (unsigned)k;
       if (row >= a.out_cap) break;
-      gd += a.dd[row];
-      if (a.dn) gn = mk3(gn.x + a.dn[3 * row], gn.y + a.dn[3 * row + 1], gn.z + a.dn[3 * row + 2]);
+      gd += (double)a.dd[row];
+      if (a.dn) gn = dadd(gn, dmk(a.dn[3 * row], a.dn[3 * row + 1], a.dn[3 * row + 2]));
     }
     uint4 qa = __ldg(a.tets + a.candA[ci]), qb = __ldg(a.tets + a.candB[ci]);
     uint32_t va[4] = {qa.x, qa.y, qa.z, qa.w}, vb[4] = {qb.x, qb.y, qb.z, qb.w};
-    f3 A[4], B[4], gA[4], gB[4];
+    d3 A[4], B[4], gA[4], gB[4];
     for (int v = 0; v < 4; ++v) {
-      A[v] = world_vertex(a.vs, va[v]);
-      B[v] = world_vertex(a.vs, vb[v]);
-      gA[v] = gB[v] = mk3(0.f, 0.f, 0.f);
+      A[v] = dof(world_vertex(a.vs, va[v]));
+      B[v] = dof(world_vertex(a.vs, vb[v]));
+      gA[v] = gB[v] = dmk(0.0, 0.0, 0.0);
     }
     int imin = r.y & 0xFF, imax = (r.y >> 8) & 0xFF;
-    f3 F0;
-    f3 m = face_m(A, r.x, F0);
-    float len = sqrtf(fdot(m, m));
-    f3 n = fs(m, 1.f / len);
-    f3 qmin = cand_point(imin, A, B), qmax = cand_point(imax, A, B);
-    cand_adj(imin, A, B, fs(n, gd), gA, gB);
-    cand_adj(imax, A, B, fs(n, -gd), gA, gB);
-    f3 gnt = fadd3(gn, fs(fsub3(qmin, qmax), gd));
-    f3 gm = fs(fsub3(gnt, fs(n, fdot(n, gnt))), 1.f / len);
+    d3 F0;
+    d3 m = face_m(A, r.x, F0);
+    double len = sqrt(ddot(m, m));
+    d3 n = dscl(m, 1.0 / len);
+    d3 qmin = cand_point(imin, A, B), qmax = cand_point(imax, A, B);
+    // depth = qmin . n - qmax . n
+    cand_adj(imin, A, B, dscl(n, gd), gA, gB);
+    cand_adj(imax, A, B, dscl(n, -gd), gA, gB);
+    d3 gnt = dadd(gn, dscl(dsub(qmin, qmax), gd));
+    d3 gm = dscl(dsub(gnt, dscl(n, ddot(n, gnt))), 1.0 / len);
     face_m_adj(A, r.x, gm, gA);
     for (int v = 0; v < 4; ++v) {
-      atomicAdd(a.grad + 3 * (size_t)va[v], gA[v].x);
-      atomicAdd(a.grad + 3 * (size_t)va[v] + 1, gA[v].y);
-      atomicAdd(a.grad + 3 * (size_t)va[v] + 2, gA[v].z);
-      atomicAdd(a.grad + 3 * (size_t)vb[v], gB[v].x);
-      atomicAdd(a.grad + 3 * (size_t)vb[v] + 1, gB[v].y);
-      atomicAdd(a.grad + 3 * (size_t)vb[v] + 2, gB[v].z);
+      atomicAdd(a.grad + 3 * (size_t)va[v], (float)gA[v].x);
+      atomicAdd(a.grad + 3 * (size_t)va[v] + 1, (float)gA[v].y);
+      atomicAdd(a.grad + 3 * (size_t)va[v] + 2, (float)gA[v].z);
+      atomicAdd(a.grad + 3 * (size_t)vb[v], (float)gB[v].x);
+      atomicAdd(a.grad + 3 * (size_t)vb[v] + 1, (float)gB[v].y);
+      atomicAdd(a.grad + 3 * (size_t)vb[v] + 2, (float)gB[v].z);
     }
   }
 }
