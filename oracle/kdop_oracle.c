@@ -569,3 +569,14 @@ void or_depth_grad_d(const double* a12, const double* b12, const or_record* rec,
     g24[12 + 3 * i] = gB[i].x; g24[12 + 3 * i + 1] = gB[i].y; g24[12 + 3 * i + 2] = gB[i].z;
   }
 }
+
+void or_frozen_batch_d(int64_t n, const double* a12, const double* b12, const or_record* rec, double* depth,
+                       double* normal) {
+  for (int64_t i = 0; i < n; ++i)
+    depth[i] = or_frozen_depth_d(a12 + 12 * i, b12 + 12 * i, rec + i, normal ? normal + 3 * i : NULL);
+}
+
+void or_depth_grad_batch_d(int64_t n, const double* a12, const double* b12, const or_record* rec, const double* gd,
+                           const double* gn, double* g24) {
+  for (int64_t i = 0; i < n; ++i) or_depth_grad_d(a12 + 12 * i, b12 + 12 * i, rec + i, gd[i], gn + 3 * i, g24 + 24 * i);
+}

@@ -110,6 +110,13 @@ double or_frozen_depth_d(const double* a12, const double* b12, const or_record* 
 void or_depth_grad_d(const double* a12, const double* b12, const or_record* rec, double gd, const double* gn,
                      double* g24);
 
+/* Batched forms of the two above over n pairs (a12/b12: n x 12, gd: n,
+ * gn: n x 3, g24: n x 24, normal: n x 3 or NULL). */
+void or_frozen_batch_d(int64_t n, const double* a12, const double* b12, const or_record* rec, double* depth,
+                       double* normal);
+void or_depth_grad_batch_d(int64_t n, const double* a12, const double* b12, const or_record* rec, const double* gd,
+                           const double* gn, double* g24);
+
 /* tiny::rotate(q, r) + p with q = (w, x, y, z) (tiny_quaternion_functions.h:149-152). */
 void or_rotate_f(const float* q, const float* p, int64_t nv, const float* xyz, float* out);
 

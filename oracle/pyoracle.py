@@ -72,6 +72,8 @@ class Oracle:
         L.or_frozen_depth_d.argtypes = [_p, _p, _p, _p]
         L.or_frozen_depth_d.restype = C.c_double
         L.or_depth_grad_d.argtypes = [_p, _p, _p, C.c_double, _p, _p]
+        L.or_frozen_batch_d.argtypes = [_i64, _p, _p, _p, _p, _p]
+        L.or_depth_grad_batch_d.argtypes = [_i64, _p, _p, _p, _p, _p, _p]
         L.or_rotate_f.argtypes = [_p, _p, _i64, _p, _p]
         L.or_sin_f.argtypes = [C.c_float]
         L.or_sin_f.restype = C.c_float
@@ -212,6 +214,27 @@ class Oracle:
         gn = _c(gn, np.float64)
         g = np.zeros(24, np.float64)
         self.lib.or_depth_grad_d(_ptr(a12), _ptr(b12), C.byref(r), float(gd), _ptr(gn), _ptr(g))
+        return g
+
+    def frozen_batch(self, a12, b12, rec):
+        """Frozen-decision depth (n,) and normal (n,3) of n pairs, double."""
+        a12, b12 = _c(a12, np.float64).reshape(-1, 12), _c(b12, np.float64).reshape(-1, 12)
+        rec = np.ascontiguousarray(rec, OR_RECORD_DTYPE)
+        n = a12.shape[0]
+        d = np.zeros(n, np.float64)
+        nrm = np.zeros((n, 3), np.float64)
+        self.lib.or_frozen_batch_d(n, _ptr(a12), _ptr(b12), _ptr(rec), _ptr(d), _ptr(nrm))
+        return d, nrm
+
+    def depth_grad_batch(self, a12, b12, rec, gd, gn):
+        """Gradient (n,24) of gd*depth + gn.normal per pair, double."""
+        a12, b12 = _c(a12, np.float64).reshape(-1, 12), _c(b12, np.float64).reshape(-1, 12)
+        rec = np.ascontiguousarray(rec, OR_RECORD_DTYPE)
+        n = a12.shape[0]
+        gd = _c(gd, np.float64).reshape(n)
+        gn = _c(gn, np.float64).reshape(n, 3)
+        g = np.zeros((n, 24), np.float64)
+        self.lib.or_depth_grad_batch_d(n, _ptr(a12), _ptr(b12), _ptr(rec), _ptr(gd), _ptr(gn), _ptr(g))
         return g
 
     def rotate(self, q, p, xyz) -> np.ndarray:

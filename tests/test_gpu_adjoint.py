@@ -21,6 +21,11 @@ H = 1e-6
 RTOL = 1e-3
 
 
+def oracle_rec_dtype():
+    from oracle.pyoracle import OR_RECORD_DTYPE
+    return OR_RECORD_DTYPE
+
+
 def run_case(ctx, oracle, sc, n_fd=1000, seed=0, w=None):
     """Loss = sum(depth^2) (+ sum(normal . w) when w is given)."""
     ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
@@ -40,36 +45,32 @@ def run_case(ctx, oracle, sc, n_fd=1000, seed=0, w=None):
     rows = ds.read_contacts()
     n_per_cand = np.bincount(rows["cand"], minlength=len(cand))
     v_off = ds.v_off
-    t_all = [m.tets.astype(np.int64) + v_off[i] for i, m in enumerate(sc.meshes)]
-    recs = {}
-    for p in np.unique(cand[n_per_cand > 0, 0]):
+    live = np.nonzero(n_per_cand > 0)[0]
+    va = np.zeros((len(live), 4), np.int64)
+    vb = np.zeros((len(live), 4), np.int64)
+    recs = np.zeros(len(live), oracle_rec_dtype())
+    for p in np.unique(cand[live, 0]):
         a, b = sc.pairs[p]
-        sel = np.nonzero((cand[:, 0] == p) & (n_per_cand > 0))[0]
-        tp = cand[sel, 1:]
+        k = np.nonzero(cand[live, 0] == p)[0]
+        tp = cand[live[k], 1:]
         A, B = sc.meshes[a], sc.meshes[b]
         xa, xb = world[v_off[a]:v_off[a + 1]], world[v_off[b]:v_off[b + 1]]
         _, rec = oracle.contacts(xa, A.tets, A.surf, xb, B.tets, B.surf, tp, "f")
-        for k, ci in enumerate(sel):
-            recs[ci] = (t_all[a][cand[ci, 1]], t_all[b][cand[ci, 2]], rec[k])
-    assert all(int(r[2]["ncontacts"]) == n_per_cand[ci] for ci, r in recs.items())
+        recs[k] = rec
+        va[k] = A.tets[tp[:, 0]].astype(np.int64) + v_off[a]
+        vb[k] = B.tets[tp[:, 1]].astype(np.int64) + v_off[b]
+    nc = n_per_cand[live].astype(np.float64)
+    assert np.array_equal(recs["ncontacts"], n_per_cand[live])
 
     X = world.astype(np.float64)
 
-    def pair_loss(va, vb, rec, ncont, Xv):
-        d, n = oracle.frozen_depth(Xv[va].ravel(), Xv[vb].ravel(), rec)
-        return ncont * (d * d + float(n @ wv))
-
     # (1) FP64 oracle gradient on every vertex
+    d, _ = oracle.frozen_batch(X[va].reshape(-1, 12), X[vb].reshape(-1, 12), recs)
+    g24 = oracle.depth_grad_batch(X[va].reshape(-1, 12), X[vb].reshape(-1, 12), recs, 2.0 * d * nc,
+                                  nc[:, None] * wv[None, :])
     g_ref = np.zeros_like(X)
-    touching = {}
-    for ci, (va, vb, rec) in recs.items():
-        nc = n_per_cand[ci]
-        d, _ = oracle.frozen_depth(X[va].ravel(), X[vb].ravel(), rec)
-        g24 = oracle.depth_grad(X[va].ravel(), X[vb].ravel(), rec, 2.0 * d * nc, nc * wv)
-        g_ref[va] += g24[:12].reshape(4, 3)
-        g_ref[vb] += g24[12:].reshape(4, 3)
-        for v in list(va) + list(vb):
-            touching.setdefault(int(v), []).append(ci)
+    np.add.at(g_ref, va.ravel(), g24[:, :12].reshape(-1, 3))
+    np.add.at(g_ref, vb.ravel(), g24[:, 12:].reshape(-1, 3))
     scale = np.abs(g_ref).max()
     err = np.abs(g_gpu - g_ref)
     bound = RTOL * np.maximum(np.abs(g_ref), 1e-2 * scale)
@@ -77,28 +78,33 @@ def run_case(ctx, oracle, sc, n_fd=1000, seed=0, w=None):
     assert not bad.any(), (bad.sum(), err[bad][:5], g_ref[bad][:5])
 
     # (2) FP64 central differences of the frozen-decision loss
+    owner = np.concatenate([np.repeat(np.arange(len(live)), 4), np.repeat(np.arange(len(live)), 4)])
+    verts = np.concatenate([va.ravel(), vb.ravel()])
+    order = np.argsort(verts, kind="stable")
+    verts_s, owner_s = verts[order], owner[order]
+    uniq, start = np.unique(verts_s, return_index=True)
+    end = np.append(start[1:], len(verts_s))
     rng = np.random.default_rng(seed)
-    verts = np.array(sorted(touching))
-    pick = rng.choice(verts, size=min(n_fd, len(verts)), replace=False)
+    pick = rng.choice(len(uniq), size=min(n_fd, len(uniq)), replace=False)
     worst = 0.0
-    for v in pick:
+    for u in pick:
+        v = uniq[u]
+        ks = np.unique(owner_s[start[u]:end[u]])
         for c in range(3):
-            lp = lm = 0.0
-            Xp = X.copy()
-            Xm = X.copy()
-            Xp[v, c] += H
-            Xm[v, c] -= H
-            for ci in touching[int(v)]:
-                va, vb, rec = recs[ci]
-                nc = n_per_cand[ci]
-                lp += pair_loss(va, vb, rec, nc, Xp)
-                lm += pair_loss(va, vb, rec, nc, Xm)
-            fd = (lp - lm) / (2 * H)
+            ls = []
+            for sgn in (1.0, -1.0):
+                a_loc, b_loc = X[va[ks]], X[vb[ks]]
+                a_loc[va[ks] == v, c] += sgn * H
+                b_loc[vb[ks] == v, c] += sgn * H
+                dd, nn = oracle.frozen_batch(a_loc.reshape(-1, 12), b_loc.reshape(-1, 12), recs[ks])
+                ls.append(float((nc[ks] * (dd * dd + nn @ wv)).sum()))
+            fd = (ls[0] - ls[1]) / (2 * H)
             e = abs(g_gpu[v, c] - fd) / max(abs(fd), 1e-2 * scale)
             worst = max(worst, e)
             assert e <= RTOL, (v, c, g_gpu[v, c], fd)
+    recs_n = len(live)
     ds.close()
-    return len(recs), len(pick), worst
+    return recs_n, len(pick), worst
 
 
 def test_adjoint_small_touching_batch(ctx, oracle):
