@@ -222,8 +222,19 @@ static void scene_free(kdop_scene* s) {
   x->stage = nullptr;
 }
 
+// A captured graph holds the buffer addresses of its capture: any
+// reallocation drops the graph (kdop_graph_launch then reports
+// KDOP_ERR_STATE until the step is captured again).
+static void drop_graph(kdop_scene* s) {
+  if (s->graph_exec) cudaGraphExecDestroy(s->graph_exec);
+  if (s->graph) cudaGraphDestroy(s->graph);
+  s->graph_exec = nullptr;
+  s->graph = nullptr;
+}
+
 static int grow_candidates(kdop_scene* s, int64_t n) {
   if (n <= s->cand_cap) return KDOP_OK;
+  drop_graph(s);
   dfree(s, &s->cand, 3 * s->cand_cap);
   dfree(s, &s->records, s->cand_cap);
   s->cand_cap = 0;
@@ -236,6 +247,7 @@ static int grow_candidates(kdop_scene* s, int64_t n) {
 
 static int grow_contacts(kdop_scene* s, int64_t n) {
   if (n <= s->contact_cap) return KDOP_OK;
+  drop_graph(s);
   dfree(s, &s->contacts, s->contact_cap);
   s->contact_cap = 0;
   if (n >= (int64_t)0xFFFFFFF0ll) return fail(s->ctx, KDOP_ERR_CAPACITY, "contact capacity above 2^32");
@@ -246,6 +258,7 @@ static int grow_contacts(kdop_scene* s, int64_t n) {
 
 static int grow_queue(kdop_scene* s, int64_t n) {
   if (n <= s->queue_cap) return KDOP_OK;
+  drop_graph(s);
   dfree(s, &s->q_items, s->queue_cap);
   dfree(s, &s->q_tags, s->queue_cap);
   s->queue_cap = 0;
@@ -259,6 +272,7 @@ static int grow_queue(kdop_scene* s, int64_t n) {
 
 static int grow_pairs(kdop_scene* s, int64_t n) {
   if (n <= s->pairs_cap) return KDOP_OK;
+  drop_graph(s);
   dfree(s, &s->pairs, s->pairs_cap);
   s->pairs_cap = 0;
   KDOP_CUDA(s->ctx, dalloc(s, &s->pairs, n));
@@ -722,6 +736,7 @@ int kdop_set_capacity(kdop_scene* s, int64_t candidates, int64_t contacts, int64
   cudaSetDevice(s->ctx->device);
   KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
   int rc = KDOP_OK;
+  if (candidates || contacts || queue) drop_graph(s);
   if (candidates) {
     dfree(s, &s->cand, 3 * s->cand_cap);
     dfree(s, &s->records, s->cand_cap);

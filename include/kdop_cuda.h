@@ -245,6 +245,8 @@ int kdop_contacts_adjoint(kdop_scene* scene, const float* d_depth, const float* 
 int kdop_set_motion(kdop_scene* scene, const float* lin_vel, const float* ang_vel, float phase_rate, int memory);
 /* Captures [motion update?] + refit(mode) + traversal + contacts into a CUDA
  * graph over the given mesh pairs.  flags bit 0: include the motion update. */
+/* Buffers must be large enough before capture (kdop_reserve): a capture
+ * holds buffer addresses, and any later reallocation drops the graph. */
 int kdop_graph_capture(kdop_scene* scene, int refit_mode, int64_t n_pairs, const uint32_t* pairs, int memory,
                        const kdop_traverse_opts* opts, int flags);
 int kdop_graph_launch(kdop_scene* scene);
