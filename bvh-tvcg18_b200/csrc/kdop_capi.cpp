@@ -70,6 +70,7 @@ struct kdop_scene_ext {
   float* stage = nullptr;
   int64_t stage_n = 0;
   std::vector<uint32_t> pairs_host;  // last traversed mesh pairs
+  std::vector<uint32_t> order_host;  // their order of processing
   int64_t graph_kernels = 0;
   kdop_traverse_opts tuned{};
   bool has_tuned = false;
@@ -210,6 +211,7 @@ static void scene_free(kdop_scene* s) {
   dfree(s, &s->ang_vel, s->n_meshes);
   dfree(s, &s->phase_dev, 1);
   dfree(s, &s->pairs, s->pairs_cap);
+  dfree(s, &s->pair_order, s->pairs_cap);
   dfree(s, &s->cand, 3 * s->cand_cap);
   dfree(s, &s->contacts, s->contact_cap);
   dfree(s, &s->records, s->cand_cap);
@@ -274,7 +276,9 @@ static int grow_pairs(kdop_scene* s, int64_t n) {
   if (n <= s->pairs_cap) return KDOP_OK;
   drop_graph(s);
   dfree(s, &s->pairs, s->pairs_cap);
+  dfree(s, &s->pair_order, s->pairs_cap);
   s->pairs_cap = 0;
+  KDOP_CUDA(s->ctx, dalloc(s, &s->pair_order, n));
   KDOP_CUDA(s->ctx, dalloc(s, &s->pairs, n));
   s->pairs_cap = n;
   return KDOP_OK;
@@ -611,6 +615,11 @@ int kdop_resolve_traverse_opts(const kdop_scene* s, const kdop_traverse_opts* o,
   p.timeout_ns = (long long)(o->timeout_ms > 0 ? o->timeout_ms : 5000) * 1000000ll;
   p.surface_filter = o->surface_filter ? 1 : 0;
   p.load_group = o->load_group > 0 ? o->load_group : d.load_group;
+  p.wave_pairs = o->wave_pairs > 0 ? o->wave_pairs : (o->wave_pairs < 0 ? -1 : d.wave_pairs);
+  p.smem_carveout = o->smem_carveout > 0 ? o->smem_carveout : (o->smem_carveout < 0 ? -1 : d.smem_carveout);
+  if (p.wave_pairs < 0) p.wave_pairs = 0;
+  if (p.smem_carveout < 0) p.smem_carveout = 0;
+  if (p.smem_carveout > 100) return KDOP_ERR_INVALID;
   if (p.block_warps > 16 || (p.stack_cap & (p.stack_cap - 1)) || p.stack_cap < 64 || p.init_chunk > 32)
     return KDOP_ERR_INVALID;
   if (p.load_group != 1 && p.load_group != 2 && p.load_group != 4) return KDOP_ERR_INVALID;
@@ -631,6 +640,8 @@ int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
   o->donate_min = 64;
   o->timeout_ms = 5000;
   o->load_group = 2;
+  o->wave_pairs = 0;
+  o->smem_carveout = 0;
   if (s) {
     kdop_scene_ext* x = ext(const_cast<kdop_scene*>(s));
     if (x->has_tuned) {
@@ -639,6 +650,8 @@ int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
       o->init_chunk = x->tuned.init_chunk;
       o->donate_min = x->tuned.donate_min;
       o->load_group = x->tuned.load_group;
+      o->wave_pairs = x->tuned.wave_pairs;
+      o->smem_carveout = x->tuned.smem_carveout;
     }
   }
   return KDOP_OK;
@@ -667,6 +680,17 @@ static int upload_pairs(kdop_scene* s, int64_t n, const uint32_t* pairs, int mem
         return fail(s->ctx, KDOP_ERR_INVALID, "mesh index out of range in pairs");
     KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->pairs, pairs, (size_t)n * 8, cudaMemcpyDeviceToDevice, s->ctx->stream));
   }
+  // largest pairs first: the traversal takes root pairs in this order
+  std::vector<uint32_t>& ord = x->order_host;
+  ord.resize((size_t)n);
+  std::vector<int64_t> size((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    uint32_t a = x->pairs_host[2 * i], b = x->pairs_host[2 * i + 1];
+    size[i] = (s->t_off[a + 1] - s->t_off[a]) + (s->t_off[b + 1] - s->t_off[b]);
+    ord[i] = (uint32_t)i;
+  }
+  std::stable_sort(ord.begin(), ord.end(), [&](uint32_t i, uint32_t j) { return size[i] > size[j]; });
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(s->pair_order, ord.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s->ctx->stream));
   return KDOP_OK;
 }
 
@@ -902,6 +926,33 @@ int kdop_graph_launch(kdop_scene* s) {
   return KDOP_OK;
 }
 
+// Times one traversal configuration: a checked warm-up run (growing the
+// buffers if needed), then `repeats` timed runs; returns milliseconds per run
+// or a negative value when the configuration cannot run.
+static float time_config(kdop_scene* s, int64_t n_pairs, const kdop::TravParams& p, int repeats, cudaEvent_t e0,
+                         cudaEvent_t e1) {
+  if (kdop::traverse_smem_bytes(p.block_warps, p.stack_cap) > s->ctx->smem_optin) return -1.f;
+  if (kdop::launch_traverse(s, n_pairs, s->pairs, p, 0) != cudaSuccess) return -1.f;
+  kdop_stats st;
+  int r = kdop_get_stats(s, &st);
+  if (r == KDOP_ERR_CAPACITY) {
+    int64_t nc = std::max<int64_t>(st.n_candidates + st.n_candidates / 4, s->cand_cap);
+    int64_t nq = (st.device_error & kdop::DEV_ERR_QUEUE_FULL) ? std::max<int64_t>(2 * s->queue_cap, 2 * st.queue_used) : 0;
+    if (kdop_reserve(s, nc, 0, nq) != KDOP_OK) return -1.f;
+    if (kdop::launch_traverse(s, n_pairs, s->pairs, p, 0) != cudaSuccess) return -1.f;
+    r = kdop_get_stats(s, &st);
+  }
+  if (r != KDOP_OK) return -1.f;
+  cudaEventRecord(e0, s->ctx->stream);
+  for (int k = 0; k < repeats; ++k) kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
+  cudaEventRecord(e1, s->ctx->stream);
+  if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  if (kdop_get_stats(s, &st) != KDOP_OK) return -1.f;
+  return ms / (float)repeats;
+}
+
 int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int memory, int repeats,
                   kdop_traverse_opts* best) {
   if (!s || n_pairs < 0 || (n_pairs > 0 && !pairs)) return KDOP_ERR_INVALID;
@@ -909,64 +960,50 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   if (repeats < 1) repeats = 1;
   int rc = upload_pairs(s, n_pairs, pairs, memory);
   if (rc != KDOP_OK) return rc;
-  const int warps[] = {8, 16};
-  const int caps[] = {256, 512, 1024};
-  const int chunks[] = {1};
-  const int donate[] = {32, 96};
-  const int groups[] = {1, 2, 4};
   cudaEvent_t e0, e1;
   KDOP_CUDA(s->ctx, cudaEventCreate(&e0));
   KDOP_CUDA(s->ctx, cudaEventCreate(&e1));
-  float best_ms = 1e30f;
-  kdop_traverse_opts bo;
-  kdop_traverse_opts_default(nullptr, &bo);
-  for (int w : warps)
-    for (int c : caps)
-      for (int ch : chunks)
-        for (int dm : donate)
-          for (int lg : groups) {
-          kdop::TravParams p;
-          p.load_group = lg;
-          p.block_warps = w;
-          p.stack_cap = c;
-          p.init_chunk = ch;
-          p.donate_min = dm;
-          p.timeout_ns = 5000000000ll;
-          p.surface_filter = 1;
-          if (kdop::traverse_smem_bytes(w, c) > s->ctx->smem_optin) continue;
-          // warm-up run, also checks the buffers are large enough
-          cudaError_t e = kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
-          if (e != cudaSuccess) continue;
-          kdop_stats st;
-          int r = kdop_get_stats(s, &st);
-          if (r == KDOP_ERR_CAPACITY) {
-            int64_t nc = std::max<int64_t>(st.n_candidates + st.n_candidates / 4, s->cand_cap);
-            int64_t nq = (st.device_error & kdop::DEV_ERR_QUEUE_FULL) ? 2 * s->queue_cap : 0;
-            rc = kdop_reserve(s, nc, 0, nq);
-            if (rc != KDOP_OK) break;
-            e = kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
-            r = kdop_get_stats(s, &st);
-          }
-          if (r != KDOP_OK) continue;
-          cudaEventRecord(e0, s->ctx->stream);
-          for (int k = 0; k < repeats; ++k) kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
-          cudaEventRecord(e1, s->ctx->stream);
-          if (cudaEventSynchronize(e1) != cudaSuccess) continue;
-          float ms = 0.f;
-          cudaEventElapsedTime(&ms, e0, e1);
-          if (kdop_get_stats(s, &st) != KDOP_OK) continue;
-          if (ms < best_ms) {
-            best_ms = ms;
-            bo.block_warps = w;
-            bo.stack_cap = c;
-            bo.init_chunk = ch;
-            bo.donate_min = dm;
-            bo.load_group = lg;
-          }
+  // coordinate descent from the defaults, two sweeps over the knobs
+  kdop_traverse_opts d;
+  kdop_traverse_opts_default(nullptr, &d);
+  kdop::TravParams cur;
+  int mode = 0;
+  kdop_resolve_traverse_opts(s, &d, cur, mode);
+  float best_ms = time_config(s, n_pairs, cur, repeats, e0, e1);
+  if (best_ms < 0.f) best_ms = 1e30f;
+  const std::vector<int> warps = {4, 8, 16}, caps = {128, 256, 512, 1024}, groups = {1, 2, 4},
+                         donate = {16, 32, 64, 128}, waves = {0, 16, 64, 128}, carve = {0, 25, 50, 100},
+                         chunk = {1, 4};
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    for (int knob = 0; knob < 7; ++knob) {
+      const std::vector<int>& vals = knob == 0 ? warps : knob == 1 ? caps : knob == 2 ? groups
+                                   : knob == 3 ? donate : knob == 4 ? waves : knob == 5 ? carve : chunk;
+      for (int v : vals) {
+        kdop::TravParams p = cur;
+        int* f = knob == 0 ? &p.block_warps : knob == 1 ? &p.stack_cap : knob == 2 ? &p.load_group
+               : knob == 3 ? &p.donate_min : knob == 4 ? &p.wave_pairs : knob == 5 ? &p.smem_carveout
+               : &p.init_chunk;
+        if (*f == v) continue;
+        *f = v;
+        float ms = time_config(s, n_pairs, p, repeats, e0, e1);
+        if (ms >= 0.f && ms < best_ms) {
+          best_ms = ms;
+          cur = p;
         }
+      }
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (best_ms >= 1e30f) return fail(s->ctx, KDOP_ERR_CUDA, "autotune: no configuration ran");
+  kdop_traverse_opts bo = d;
+  bo.block_warps = cur.block_warps;
+  bo.stack_cap = cur.stack_cap;
+  bo.init_chunk = cur.init_chunk;
+  bo.donate_min = cur.donate_min;
+  bo.load_group = cur.load_group;
+  bo.wave_pairs = cur.wave_pairs;
+  bo.smem_carveout = cur.smem_carveout;
   kdop_scene_ext* x = ext(s);
   x->tuned = bo;
   x->has_tuned = true;

@@ -52,6 +52,8 @@ struct TravParams {
   long long timeout_ns;
   int surface_filter;
   int load_group;
+  int wave_pairs;
+  int smem_carveout;
 };
 
 }  // namespace kdop
@@ -99,6 +101,7 @@ struct kdop_scene {
 
   // traversal / contacts buffers
   uint2* pairs = nullptr;
+  uint32_t* pair_order = nullptr;  // pair indices by decreasing size (tets of A + tets of B)
   int64_t pairs_cap = 0;
   uint32_t* cand = nullptr;  // 3 * cand_cap: A tets | B tets | pair ids
   int64_t cand_cap = 0;

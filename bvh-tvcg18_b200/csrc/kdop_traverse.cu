@@ -29,6 +29,7 @@
 //   * termination: a global count of outstanding work units reaches zero;
 //     every wait is bounded by a time limit after which the kernel records
 //     DEV_ERR_TIMEOUT and returns (no unbounded spin).
+#include <algorithm>
 #include <mutex>
 
 #include "kdop_device.cuh"
@@ -54,12 +55,14 @@ struct TravArgs {
   int surface_filter;
   long long timeout_ns;
   unsigned n_meshes;
+  const uint32_t* __restrict__ order;  // root pair i -> pair index (NULL: identity)
 };
 
 // Device buffers one traversal works in: pairs (input), candidates (output),
 // work queue and control block (scratch).
 struct TravBuffers {
   const uint2* pairs;
+  const uint32_t* order;  // processing order of the pairs, or NULL
   uint32_t* cand;  // 3 * cand_cap: A tets | B tets | pair ids
   int64_t cand_cap;
   uint4* q_items;
@@ -208,6 +211,7 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
             // root test (kdop_tandem_traversal.h:164), then the traversal's own
             // test of the root pair (:42), both counted as the reference does.
             pid = pair_base + base + lane;
+            if (a.order) pid = a.order[pid];
             uint2 mp = a.pairs[pid];
             uint32_t ra = NO_NODE, rb = NO_NODE;
             if (mp.x < a.n_meshes && mp.y < a.n_meshes) {
@@ -489,6 +493,9 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
   size_t smem = traverse_smem_bytes(p.block_warps, p.stack_cap);
   cudaError_t e = prepare_k<K>(smem);
   if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(traverse_kernel<K, G>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           p.smem_carveout > 0 ? p.smem_carveout : -1);
+  if (e != cudaSuccess) return e;
   int per_sm = 0;
   e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_kernel<K, G>, threads, smem);
   if (e != cudaSuccess) return e;
@@ -499,6 +506,7 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
   a.surf = s->surf;
   a.root = s->root_dev;
   a.pairs = b.pairs;
+  a.order = b.order;
   a.candA = b.cand;
   a.candB = b.cand + b.cand_cap;
   a.candP = b.cand + 2 * b.cand_cap;
@@ -514,9 +522,16 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
   a.surface_filter = p.surface_filter;
   a.timeout_ns = p.timeout_ns;
   if (!plain) {
-    trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)n_pairs, 0u, 1);
-    traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
-    s->ctx->launches += 2;
+    // waves of wave_pairs root pairs (largest first), or all at once
+    int64_t wave = p.wave_pairs > 0 ? p.wave_pairs : n_pairs;
+    if (wave < 1) wave = 1;
+    for (int64_t off = 0; off < n_pairs || off == 0; off += wave) {
+      int64_t n = std::min<int64_t>(wave, n_pairs - off);
+      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)std::max<int64_t>(n, 0), (unsigned)off, off == 0);
+      traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
+      s->ctx->launches += 2;
+      if (n_pairs == 0) break;
+    }
   } else {
     for (int64_t i = 0; i < n_pairs; ++i) {
       trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 1u, (unsigned)i, i == 0 ? 1 : 0);
@@ -558,6 +573,7 @@ static cudaError_t traverse_buffers(kdop_scene* s, int64_t n_pairs, const TravBu
 cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int plain) {
   TravBuffers b;
   b.pairs = pairs;
+  b.order = s->pair_order;
   b.cand = s->cand;
   b.cand_cap = s->cand_cap;
   b.q_items = s->q_items;
@@ -631,6 +647,7 @@ extern "C" int kdop_traverse_noalloc(kdop_scene* s, int64_t n_pairs, const uint3
   }
   TravBuffers b;
   b.pairs = reinterpret_cast<const uint2*>(pairs);
+  b.order = nullptr;
   b.cand = candidates;
   b.cand_cap = cap;
   b.ctl = reinterpret_cast<TravCtl*>(base);

@@ -200,7 +200,9 @@ def test_surface_filter_off_matches_unfiltered_oracle(ctx, oracle):
 @pytest.mark.parametrize("cfg", [dict(block_warps=4, stack_cap=64, donate_min=8, load_group=1),
                                  dict(block_warps=16, stack_cap=1024, init_chunk=4, donate_min=128, load_group=4),
                                  dict(block_warps=2, stack_cap=128, init_chunk=32, donate_min=16, load_group=2),
-                                 dict(block_warps=8, stack_cap=256, load_group=4)])
+                                 dict(block_warps=8, stack_cap=256, load_group=4),
+                                 dict(wave_pairs=3, smem_carveout=50, load_group=4),
+                                 dict(wave_pairs=1, smem_carveout=100, stack_cap=128)])
 def test_tuning_knobs_do_not_change_results(ctx, oracle, cfg):
     sc = scenes.small_batch(n_pairs=10, n_lo=3, n_hi=7, seed=21)
     worlds = scene_world(oracle, sc)
