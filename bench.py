@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample, seconds")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--opts", default="", help="traversal options key=value,... (skips the autotuner)")
     return ap.parse_args()
 
 
@@ -256,9 +257,12 @@ def run_cuda(args):
     ds.refit(kd.REFIT_POSE)
     st = ds.traverse_sync(sc.pairs, contacts=True)
     tuned = None
-    if not args.no_autotune:
-        tuned = ds.autotune(sc.pairs, repeats=2).as_dict()
-    opts = ds.default_opts()
+    if args.opts:
+        opts = ds.opts(**{k: int(v) for k, v in (kv.split("=") for kv in args.opts.split(","))})
+    else:
+        if not args.no_autotune:
+            tuned = ds.autotune(sc.pairs, repeats=2).as_dict()
+        opts = ds.default_opts()
     st = ds.traverse_sync(sc.pairs, opts, contacts=True)
     tests_per_step = st.n_tests
     ds.reserve(candidates=int(st.n_candidates * 1.2) + 1024, contacts=int(st.n_contacts * 1.2) + 1024,
@@ -310,25 +314,35 @@ def run_cuda(args):
     achieved = alg_bytes / (trav_ms * 1e-3) / 1e9
     traffic = ncu_traffic("traverse_config3.md")
 
-    # plain: one traversal launch per mesh pair, same trees and descent rule
+    # plain: one traversal launch per mesh pair, same trees and descent rule;
+    # the faster of the default and the batched-tuned launch shape
     plain = None
     if not args.no_plain:
-        popts = ds.opts(mode=kd.TRAVERSE_PLAIN)
-        ds.traverse_sync(sc.pairs, popts)
-        pt = []
-        for _ in range(2):
-            a0 = torch.cuda.Event(enable_timing=True)
-            a1 = torch.cuda.Event(enable_timing=True)
-            a0.record(stream)
-            ds.traverse(sc.pairs, popts)
-            a1.record(stream)
-            a1.synchronize()
-            pt.append(a0.elapsed_time(a1))
-        pst = ds.stats()
-        assert pst.n_tests == tests_per_step
-        plain_ms = min(pt)
+        best = None
+        for name in ("default", "tuned"):
+            if name == "default":
+                popts = kd.TraverseOpts()
+                ds.lib.kdop_traverse_opts_default(None, popts)
+            else:
+                popts = kd.TraverseOpts.from_buffer_copy(opts)
+            popts.mode = kd.TRAVERSE_PLAIN
+            ds.traverse_sync(sc.pairs, popts)
+            pt = []
+            for _ in range(2):
+                a0 = torch.cuda.Event(enable_timing=True)
+                a1 = torch.cuda.Event(enable_timing=True)
+                a0.record(stream)
+                ds.traverse(sc.pairs, popts)
+                a1.record(stream)
+                a1.synchronize()
+                pt.append(a0.elapsed_time(a1))
+            pst = ds.stats()
+            assert pst.n_tests == tests_per_step
+            if best is None or min(pt) < best[0]:
+                best = (min(pt), name, popts.as_dict())
+        plain_ms = best[0]
         plain = {"traversal_ms": plain_ms, "tests_per_s": tests_per_step / (plain_ms * 1e-3),
-                 "batched_speedup": plain_ms / trav_ms}
+                 "batched_speedup": plain_ms / trav_ms, "launch_shape": best[1], "opts": best[2]}
 
     # e2e: through the public API with host buffers; per step the world
     # positions of all meshes go host->device (pinned) and the contacts and
