@@ -76,6 +76,12 @@ __device__ __forceinline__ unsigned long long global_ns() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+// 256-bit read-only load of two consecutive float4 chunks (p 32-byte aligned).
+__device__ __forceinline__ void ldg256(const float4* p, float4& x, float4& y) {
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(x.x), "=f"(x.y), "=f"(x.z), "=f"(x.w), "=f"(y.x), "=f"(y.y), "=f"(y.z), "=f"(y.w)
+               : "l"(p));
+}
 __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(const volatile unsigned*)p; }
 __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
 
@@ -133,19 +139,38 @@ struct Expand {
     const float4* pa = nodes + (int64_t)a0 * L::NW;
     const float4* pb = nodes + (int64_t)b0 * L::NW;
     stA[0] = stA[1] = enA[0] = enA[1] = stB[0] = stB[1] = enB[0] = enB[1] = 0;
+    // Records of an even number of chunks start on 32-byte boundaries, so
+    // two chunks come in one 256-bit load (half the L1 wavefronts).
+    constexpr bool kWide = (L::NW % 2 == 0) && (G % 2 == 0);
 #pragma unroll
     for (int j0 = 0; j0 < L::NW; j0 += G) {
       if (sep == 0xF) break;
       float4 A0[G], A1[G], B0[G], B1[G];
+      if (kWide) {
 #pragma unroll
-      for (int g = 0; g < G; ++g) {
-        if (j0 + g < L::NW) {
-          A0[g] = __ldg(pa + j0 + g);
-          B0[g] = __ldg(pb + j0 + g);
-          A1[g] = A0[g];
-          B1[g] = B0[g];
-          if (na == 2) A1[g] = __ldg(pa + L::NW + j0 + g);
-          if (nb == 2) B1[g] = __ldg(pb + L::NW + j0 + g);
+        for (int g = 0; g < G; g += 2) {
+          if (j0 + g < L::NW) {
+            ldg256(pa + j0 + g, A0[g], A0[g + 1]);
+            ldg256(pb + j0 + g, B0[g], B0[g + 1]);
+            A1[g] = A0[g];
+            A1[g + 1] = A0[g + 1];
+            B1[g] = B0[g];
+            B1[g + 1] = B0[g + 1];
+            if (na == 2) ldg256(pa + L::NW + j0 + g, A1[g], A1[g + 1]);
+            if (nb == 2) ldg256(pb + L::NW + j0 + g, B1[g], B1[g + 1]);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int g = 0; g < G; ++g) {
+          if (j0 + g < L::NW) {
+            A0[g] = __ldg(pa + j0 + g);
+            B0[g] = __ldg(pb + j0 + g);
+            A1[g] = A0[g];
+            B1[g] = B0[g];
+            if (na == 2) A1[g] = __ldg(pa + L::NW + j0 + g);
+            if (nb == 2) B1[g] = __ldg(pb + L::NW + j0 + g);
+          }
         }
       }
 #pragma unroll
