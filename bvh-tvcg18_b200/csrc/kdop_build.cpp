@@ -164,8 +164,11 @@ struct TreeLevels {
   std::vector<std::vector<std::pair<uint32_t, uint32_t> > > levels;  // (first, last) per node
 };
 
-void build_levels(const float* xyz, int64_t nt, const uint32_t* tets, TreeLevels& tl) {
-  morton_order(xyz, nt, tets, tl.perm);
+void build_levels(const float* xyz, int64_t nt, const uint32_t* tets, const uint32_t* order, TreeLevels& tl) {
+  if (order)
+    tl.perm.assign(order, order + nt);
+  else
+    morton_order(xyz, nt, tets, tl.perm);
   tl.levels.clear();
   if (nt <= 0) return;
   std::vector<std::pair<uint32_t, uint32_t> > cur(1, std::make_pair(0u, (uint32_t)(nt - 1)));
@@ -211,11 +214,11 @@ void parallel_for(int n, F fn) {
 
 int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t>& n_verts,
                  const std::vector<const uint32_t*>& tets, const std::vector<int64_t>& n_tets,
-                 const std::vector<int64_t>& t_off, ForestBuild& out) {
+                 const std::vector<const uint32_t*>& orders, const std::vector<int64_t>& t_off, ForestBuild& out) {
   (void)n_verts;
   int nm = (int)tets.size();
   std::vector<TreeLevels> trees((size_t)nm);
-  parallel_for(nm, [&](int m) { build_levels(xyz[m], n_tets[m], tets[m], trees[m]); });
+  parallel_for(nm, [&](int m) { build_levels(xyz[m], n_tets[m], tets[m], orders[m], trees[m]); });
   int depth = 0;
   for (int m = 0; m < nm; ++m) depth = std::max(depth, (int)trees[m].levels.size());
   // pre[m][d]: nodes of trees < m at level d

@@ -298,6 +298,15 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
     for (int64_t i = 0; i < 4 * d.n_tets; ++i)
       if ((int64_t)d.tets[i] >= d.n_verts)
         return fail(ctx, KDOP_ERR_INVALID, "tet vertex index out of range in mesh " + std::to_string(m));
+    if (d.leaf_order) {
+      std::vector<char> seen((size_t)d.n_tets, 0);
+      for (int64_t i = 0; i < d.n_tets; ++i) {
+        uint32_t t = d.leaf_order[i];
+        if ((int64_t)t >= d.n_tets || seen[t])
+          return fail(ctx, KDOP_ERR_INVALID, "leaf_order is not a permutation in mesh " + std::to_string(m));
+        seen[t] = 1;
+      }
+    }
     nv += d.n_verts;
     nt += d.n_tets;
   }
@@ -326,14 +335,16 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
   std::vector<const float*> xyz((size_t)n_meshes);
   std::vector<const uint32_t*> tets((size_t)n_meshes);
   std::vector<int64_t> nvs((size_t)n_meshes), nts((size_t)n_meshes);
+  std::vector<const uint32_t*> orders((size_t)n_meshes);
   for (int m = 0; m < n_meshes; ++m) {
     xyz[m] = meshes[m].xyz;
     tets[m] = meshes[m].tets;
+    orders[m] = meshes[m].leaf_order;
     nvs[m] = meshes[m].n_verts;
     nts[m] = meshes[m].n_tets;
   }
   kdop::ForestBuild fb;
-  if (kdop::build_forest(xyz, nvs, tets, nts, s->t_off, fb) != 0) {
+  if (kdop::build_forest(xyz, nvs, tets, nts, orders, s->t_off, fb) != 0) {
     delete box;
     return fail(ctx, KDOP_ERR_INVALID, "scene too large for 31-bit node indices");
   }

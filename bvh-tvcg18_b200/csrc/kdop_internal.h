@@ -139,7 +139,7 @@ struct ForestBuild {
 // meshes: tet counts and concatenated (global-vertex) tets; t_off per mesh.
 int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t>& n_verts,
                  const std::vector<const uint32_t*>& tets, const std::vector<int64_t>& n_tets,
-                 const std::vector<int64_t>& t_off, ForestBuild& out);
+                 const std::vector<const uint32_t*>& orders, const std::vector<int64_t>& t_off, ForestBuild& out);
 void morton_order(const float* xyz, int64_t n_tets, const uint32_t* tets, std::vector<uint32_t>& perm);
 void surface_map(int64_t n_tets, const uint32_t* tets, uint8_t* surf);
 

@@ -38,7 +38,7 @@ class KdopError(RuntimeError):
 
 class MeshDesc(C.Structure):
     _fields_ = [("n_verts", C.c_int64), ("xyz", C.c_void_p), ("n_tets", C.c_int64), ("tets", C.c_void_p),
-                ("surface", C.c_void_p)]
+                ("surface", C.c_void_p), ("leaf_order", C.c_void_p)]
 
 
 class SceneInfo(C.Structure):
@@ -219,7 +219,10 @@ class DeviceScene:
             tets = np.ascontiguousarray(m.tets, np.uint32)
             surf = np.ascontiguousarray(m.surf, np.uint8) if (surface and m.surf is not None) else None
             self._keep += [xyz, tets, surf]
-            descs[i] = MeshDesc(xyz.shape[0], _ptr(xyz), tets.shape[0], _ptr(tets), _ptr(surf))
+            order = getattr(m, "leaf_order", None)
+            order = None if order is None else np.ascontiguousarray(order, np.uint32)
+            self._keep.append(order)
+            descs[i] = MeshDesc(xyz.shape[0], _ptr(xyz), tets.shape[0], _ptr(tets), _ptr(surf), _ptr(order))
             self.v_off[i + 1] = self.v_off[i] + xyz.shape[0]
             self.t_off[i + 1] = self.t_off[i] + tets.shape[0]
         h = C.c_void_p()

@@ -86,12 +86,16 @@ typedef struct {
   int64_t n_tets;
   const uint32_t* tets;    /* host, n_tets * 4, mesh-local vertex indices */
   const uint8_t* surface;  /* host, n_tets boundary-face bits, or NULL to compute them */
+  const uint32_t* leaf_order; /* host, n_tets: the tets in leaf order (a permutation), or
+                                 NULL for the Morton order of the rest positions */
 } kdop_mesh_desc;
 
 /* Builds one tree per mesh on the host with the reference's topology
  * (Morton order of tet centroids, index-median split, 1 tet per leaf: the
  * one-chunk tree of make_tree with mem_bytes = SIZE_MAX) and uploads meshes
- * and trees.  Leaves keep the caller's tet numbering. */
+ * and trees.  Leaves keep the caller's tet numbering.  A leaf_order of
+ * 0, 1, ..., n_tets-1 reproduces make_tree's tree of a mesh as given (the
+ * reference reorders meshes before building, kdop_mesh_reorder.h:364-387). */
 int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* meshes, kdop_scene** out);
 int kdop_scene_destroy(kdop_scene* scene);
 
