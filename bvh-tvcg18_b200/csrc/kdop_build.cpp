@@ -233,9 +233,14 @@ int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t
     }
     tot[d] = acc;
   }
+  // Twin records need every sibling pair at an even index: levels >= 1 hold
+  // whole sibling pairs, so an even root level suffices (one padding node,
+  // a copy of the first root's topology, when the count is odd).
+  const int64_t n_roots = depth > 0 ? tot[0] : 0;
+  if (n_roots & 1) tot[0] += 1;
   for (int d = 0; d < depth; ++d) out.level_off[d + 1] = out.level_off[d] + tot[d];
   int64_t nn = out.level_off[depth];
-  if (nn >= (int64_t)LEAF_BIT_HOST) return -1;
+  if (nn >= (int64_t)(LEAF_BIT_HOST >> 1)) return -1;  // node indices use 30 bits
   out.topo.assign(2 * (size_t)nn, 0);
   out.root.assign((size_t)nm, 0xFFFFFFFFu);
   out.depth = depth > 0 ? depth - 1 : 0;
@@ -263,6 +268,12 @@ int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t
     std::vector<uint32_t>().swap(tl.perm);
     std::vector<std::vector<std::pair<uint32_t, uint32_t> > >().swap(tl.levels);
   });
+  if (n_roots & 1) {
+    // the padding slot ending the root level repeats the first root's
+    // topology (refitted like it, never reached by a traversal)
+    out.topo[2 * (size_t)n_roots] = out.topo[0];
+    out.topo[2 * (size_t)n_roots + 1] = out.topo[1];
+  }
   return 0;
 }
 

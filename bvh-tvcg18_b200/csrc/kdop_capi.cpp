@@ -346,7 +346,7 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
   kdop::ForestBuild fb;
   if (kdop::build_forest(xyz, nvs, tets, nts, orders, s->t_off, fb) != 0) {
     delete box;
-    return fail(ctx, KDOP_ERR_INVALID, "scene too large for 31-bit node indices");
+    return fail(ctx, KDOP_ERR_INVALID, "scene too large for 30-bit node indices");
   }
   s->level_off = fb.level_off;
   s->root = fb.root;
@@ -477,25 +477,28 @@ int kdop_read_tree(kdop_scene* s, int mesh, int64_t cap, float* vol, int64_t* te
   std::vector<float> rec((size_t)(s->nn * s->NW * 4));
   KDOP_CUDA(s->ctx, cudaMemcpyAsync(rec.data(), s->nodes, rec.size() * 4, cudaMemcpyDeviceToHost, s->ctx->stream));
   KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
-  const int W = s->NW * 4;
   const int tw = s->K;  // word index of `start`
   std::vector<uint32_t> stack(1, s->root[mesh]);
   int64_t k = 0;
   while (!stack.empty()) {
     uint32_t n = stack.back();
     stack.pop_back();
-    const float* r = &rec[(size_t)n * W];
-    uint32_t st, en;
-    std::memcpy(&st, r + tw, 4);
-    std::memcpy(&en, r + tw + 1, 4);
+    // chunk j of node n sits at float4 2 NW (n / 2) + 2 j + n % 2 (twin records)
+    float r[32];  // NW <= 7 chunks
+    for (int j = 0; j < s->NW; ++j)
+      std::memcpy(r + 4 * j, &rec[4 * (size_t)((int64_t)(n >> 1) * 2 * s->NW + 2 * j + (n & 1))], 16);
+    // topology words: leaf (LEAF_BIT | flags | own index, tet), internal (c, c + 1)
+    uint32_t w0, w1;
+    std::memcpy(&w0, r + tw, 4);
+    std::memcpy(&w1, r + tw + 1, 4);
     if (k >= *n_nodes) return fail(s->ctx, KDOP_ERR_STATE, "tree walk overran the node count");
     std::memcpy(vol + k * s->K, r, (size_t)s->K * 4);
-    if (st == en) {
-      tet[k] = (int64_t)st - s->t_off[mesh];
+    if (w0 & kdop::LEAF_BIT_HOST) {
+      tet[k] = (int64_t)w1 - s->t_off[mesh];
     } else {
       tet[k] = -1;
-      stack.push_back(en);
-      stack.push_back(st);
+      stack.push_back(w1);
+      stack.push_back(w0);
     }
     ++k;
   }
@@ -645,12 +648,12 @@ int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
   std::memset(o, 0, sizeof(*o));
   o->mode = KDOP_TRAVERSE_BATCHED;
   o->surface_filter = 1;
-  o->block_warps = 8;
+  o->block_warps = 16;
   o->stack_cap = 512;
   o->init_chunk = 1;
-  o->donate_min = 64;
+  o->donate_min = 128;
   o->timeout_ms = 5000;
-  o->load_group = 2;
+  o->load_group = 4;
   o->wave_pairs = 0;
   o->smem_carveout = 0;
   if (s) {
@@ -983,7 +986,7 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   float best_ms = time_config(s, n_pairs, cur, repeats, e0, e1);
   if (best_ms < 0.f) best_ms = 1e30f;
   const std::vector<int> warps = {4, 8, 16}, caps = {128, 256, 512, 1024}, groups = {1, 2, 4},
-                         donate = {16, 32, 64, 128}, waves = {0, 16, 64, 128}, carve = {0, 25, 50, 100},
+                         donate = {32, 64, 128, 256}, waves = {0, 16, 64, 128}, carve = {0, 25, 50, 100},
                          chunk = {1, 4};
   for (int sweep = 0; sweep < 2; ++sweep) {
     for (int knob = 0; knob < 7; ++knob) {

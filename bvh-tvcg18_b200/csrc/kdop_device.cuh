@@ -15,19 +15,37 @@
 namespace kdop {
 
 constexpr uint32_t LEAF_BIT = 0x80000000u;
+constexpr uint32_t SURF_BIT = 0x40000000u;   // leaf word: the tet has a boundary face
+constexpr uint32_t NODE_MASK = 0x3FFFFFFFu;  // node index bits of a word
 constexpr uint32_t NO_NODE = 0xFFFFFFFFu;
 
 // ---- node record ------------------------------------------------------------
 // K floats of slabs (lo_s, hi_s interleaved, s = 0..K/2-1, in direction-table
-// order), then the two topology words (start, end) of kdop_tree.h:15-75
-// (leaf <=> start == end, start = global tet index; internal: children are the
-// nodes start and end = start + 1), padded to whole float4 chunks.
+// order), then two topology words, padded to whole float4 chunks.  The words
+// carry kdop_tree.h:15-75's (m_start, m_end) in a form the traversal can push
+// without decoding:
+//   internal node: (c, c + 1), its children c (even) and c + 1;
+//   leaf:          (LEAF_BIT | SURF_BIT if the tet has a boundary face | the
+//                   leaf's own node index, global tet index).
+// So word 0 of a child is exactly the deque entry that stands for it (its
+// first child, or itself flagged as a leaf).  Node indices use 30 bits.
+//
+// Twin records: siblings always sit at node indices 2t, 2t + 1 (the forest
+// pads its root level to an even count), and the two records of twin t are
+// stored chunk-interleaved: chunk j of node 2t + s is float4 2 NW t + 2 j + s.
+// Chunk j of both siblings is therefore one aligned 32-byte word, and a whole
+// twin is 2 NW float4 of consecutive memory.
 template <int K>
 struct NodeLayout {
   static constexpr int NS = K / 2;                 // slabs
   static constexpr int NW = (K + 2 + 3) / 4;       // float4 chunks per record
   static constexpr int TOPO_CHUNK = K / 4;         // chunk holding (start, end)
   static constexpr bool TOPO_ZW = (K % 4) == 2;    // (start,end) in .z,.w (else .x,.y)
+  // float4 index of chunk j of node n
+  __host__ __device__ static constexpr int64_t at(int64_t n, int j) { return (n >> 1) * (2 * NW) + 2 * j + (n & 1); }
+  // topology words of a record's topology chunk
+  __device__ static __forceinline__ uint32_t word0(const float4& c) { return __float_as_uint(TOPO_ZW ? c.z : c.x); }
+  __device__ static __forceinline__ uint32_t word1(const float4& c) { return __float_as_uint(TOPO_ZW ? c.w : c.y); }
 };
 
 // ---- separately rounded float arithmetic --------------------------------------

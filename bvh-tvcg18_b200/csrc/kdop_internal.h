@@ -21,22 +21,30 @@ struct DirTable {
   float d[13][3];
 };
 
-// Device-side control block of one traversal (+ contact generation).
+// Device-side control block of one traversal (+ contact generation).  The counters that every warp updates or polls
+// while the traversal runs sit on 128-byte lines of their own, so that atomics
+// and polls on one do not queue behind traffic on another in the same L2 slice.
 struct TravCtl {
   unsigned long long tests;          // node-pair tests
   unsigned long long leaf_overlaps;  // overlapping leaf pairs before the surface filter
-  unsigned int n_cand;               // candidates emitted (may exceed capacity)
-  unsigned int init_head;            // root pairs claimed
-  unsigned int q_head;               // queue slots claimed by idle warps
-  unsigned int q_tail;               // queue slots reserved by producers
-  int work;                          // outstanding work units; 0 = traversal finished
   unsigned int error;                // DEV_ERR_* bits
   unsigned int n_contacts;           // contacts emitted (may exceed capacity)
   unsigned int n_init;               // root pairs in this launch
   unsigned int pair_base;            // pair index of the first root pair
   unsigned int max_stack;            // deepest warp stack seen
-  unsigned int pad[2];
+  unsigned int pad0[23];
+  unsigned int n_cand;               // candidates emitted (may exceed capacity)
+  unsigned int pad1[31];
+  unsigned int init_head;            // root pairs claimed
+  unsigned int pad2[31];
+  unsigned int q_head;               // queue slots claimed by idle warps
+  unsigned int pad3[31];
+  unsigned int q_tail;               // queue slots reserved by producers
+  unsigned int pad4[31];
+  int work;                          // outstanding work units; 0 = traversal finished
+  unsigned int pad5[31];
 };
+static_assert(sizeof(TravCtl) == 768, "one 128-byte line per hot counter");
 
 enum : unsigned int {
   DEV_ERR_TIMEOUT = 1u,

@@ -8,10 +8,11 @@
 // (cl/kernels/kdop_cl_refit_tree.cl:17-168).
 //
 // Here the forest is stored level by level, so one launch refits one level of
-// every tree at once, deepest level first.  Thread t handles float4 chunk
-// t % NW of node t / NW: consecutive threads write consecutive 16-byte words
-// (fully coalesced stores) and read the same chunk of the two adjacent
-// children.  Leaves transform their vertices on the fly when the scene is in
+// every tree at once, deepest level first.  Thread t writes float4 slot t of
+// the level's twin records (chunk j of node n at slot 2 NW (n / 2) + 2 j +
+// n % 2): consecutive threads write consecutive 16-byte words (fully coalesced
+// stores), and an internal node reads chunk j of its two children, the twin
+// record below it, as one 32-byte load.  Leaves transform their vertices on the fly when the scene is in
 // pose or deform mode (narrow_update_kdop_bvh.h:154-165 fused into the leaf
 // pass, so no world-vertex array is written).  The upper levels, too small to
 // fill the GPU, are refitted by one block that walks them with block barriers.
@@ -23,12 +24,11 @@ template <int K>
 __device__ __forceinline__ float4 refit_chunk(const float4* nodes, int64_t node, int j, const uint4* __restrict__ tets,
                                               const VertexSource& vs, const DirTable& dt, bool use_ldg) {
   using L = NodeLayout<K>;
-  float4 tc = use_ldg ? __ldg(nodes + node * L::NW + L::TOPO_CHUNK) : nodes[node * L::NW + L::TOPO_CHUNK];
-  uint32_t start = __float_as_uint(L::TOPO_ZW ? tc.z : tc.x);
-  uint32_t end = __float_as_uint(L::TOPO_ZW ? tc.w : tc.y);
+  float4 tc = use_ldg ? __ldg(nodes + L::at(node, L::TOPO_CHUNK)) : nodes[L::at(node, L::TOPO_CHUNK)];
+  const uint32_t w0 = L::word0(tc), w1 = L::word1(tc);
   float w[4];
-  if (start == end) {
-    uint4 t = __ldg(tets + start);
+  if (w0 & LEAF_BIT) {
+    uint4 t = __ldg(tets + w1);
     f3 p[4] = {world_vertex(vs, t.x), world_vertex(vs, t.y), world_vertex(vs, t.z), world_vertex(vs, t.w)};
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -50,8 +50,15 @@ __device__ __forceinline__ float4 refit_chunk(const float4* nodes, int64_t node,
       }
     }
   } else {
-    float4 a = use_ldg ? __ldg(nodes + (int64_t)start * L::NW + j) : nodes[(int64_t)start * L::NW + j];
-    float4 b = use_ldg ? __ldg(nodes + (int64_t)end * L::NW + j) : nodes[(int64_t)end * L::NW + j];
+    // chunk j of the children w0, w0 + 1: one aligned 32-byte word of their twin
+    float4 a, b;
+    if (use_ldg) {
+      a = __ldg(nodes + L::at(w0, j));
+      b = __ldg(nodes + L::at(w0, j) + 1);
+    } else {
+      a = nodes[L::at(w0, j)];
+      b = nodes[L::at(w0, j) + 1];
+    }
     // lo: min(A.lo, B.lo) = (B < A) ? B : A ; hi: max(A.hi, B.hi) = (A < B) ? B : A
     w[0] = smin(a.x, b.x);
     w[1] = smax(a.y, b.y);
@@ -85,10 +92,10 @@ __global__ void __launch_bounds__(256) refit_level_kernel(float4* nodes, int64_t
   using L = NodeLayout<K>;
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= count * L::NW) return;
-  int64_t node = begin + t / L::NW;
-  int j = (int)(t % L::NW);
-  float4 o = refit_chunk<K>(nodes, node, j, tets, vs, dt, true);
-  nodes[node * L::NW + j] = o;
+  int64_t f = begin * L::NW + t;  // float4 slot (begin and count are even)
+  int64_t node = 2 * (f / (2 * L::NW)) + (f & 1);
+  int j = (int)((f % (2 * L::NW)) >> 1);
+  nodes[f] = refit_chunk<K>(nodes, node, j, tets, vs, dt, true);
 }
 
 // Levels [0, last] of the forest, deepest first, by a single block.
@@ -98,28 +105,34 @@ __global__ void __launch_bounds__(1024) refit_tail_kernel(float4* nodes, const i
                                                           VertexSource vs, DirTable dt) {
   using L = NodeLayout<K>;
   for (int d = last; d >= 0; --d) {
-    int64_t b = level_off[d], n = (level_off[d + 1] - b) * L::NW;
-    for (int64_t t = threadIdx.x; t < n; t += blockDim.x) {
-      int64_t node = b + t / L::NW;
-      int j = (int)(t % L::NW);
-      float4 o = refit_chunk<K>(nodes, node, j, tets, vs, dt, false);
-      nodes[node * L::NW + j] = o;
+    int64_t b = level_off[d] * L::NW, e = level_off[d + 1] * L::NW;
+    for (int64_t f = b + threadIdx.x; f < e; f += blockDim.x) {
+      int64_t node = 2 * (f / (2 * L::NW)) + (f & 1);
+      int j = (int)((f % (2 * L::NW)) >> 1);
+      nodes[f] = refit_chunk<K>(nodes, node, j, tets, vs, dt, false);
     }
     __syncthreads();
   }
 }
 
-// Topology words (start, end) into the node records, slabs zeroed.
+// Topology words into the node records, slabs zeroed.  topo holds the
+// reference's (m_start, m_end) per node (leaf <=> start == end = tet).
 template <int K>
-__global__ void write_topology_kernel(float4* nodes, int64_t nn, const uint32_t* __restrict__ topo) {
+__global__ void write_topology_kernel(float4* nodes, int64_t nn, const uint32_t* __restrict__ topo,
+                                      const uint8_t* __restrict__ surf) {
   using L = NodeLayout<K>;
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nn * L::NW) return;
-  int64_t node = t / L::NW;
-  int j = (int)(t % L::NW);
+  int64_t node = 2 * (t / (2 * L::NW)) + (t & 1);
+  int j = (int)((t % (2 * L::NW)) >> 1);
   float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
   if (j == L::TOPO_CHUNK) {
-    float a = __uint_as_float(topo[2 * node]), b = __uint_as_float(topo[2 * node + 1]);
+    uint32_t st = topo[2 * node], en = topo[2 * node + 1];
+    if (st == en) {
+      en = st;
+      st = LEAF_BIT | (surf[en] ? SURF_BIT : 0u) | (uint32_t)node;
+    }
+    float a = __uint_as_float(st), b = __uint_as_float(en);
     if (L::TOPO_ZW) {
       o.z = a;
       o.w = b;
@@ -259,7 +272,7 @@ template <int K>
 static cudaError_t topo_impl(kdop_scene* s, const uint32_t* topo) {
   int64_t items = s->nn * NodeLayout<K>::NW;
   if (items == 0) return cudaSuccess;
-  write_topology_kernel<K><<<(unsigned)((items + 255) / 256), 256, 0, s->ctx->stream>>>(s->nodes, s->nn, topo);
+  write_topology_kernel<K><<<(unsigned)((items + 255) / 256), 256, 0, s->ctx->stream>>>(s->nodes, s->nn, topo, s->surf);
   s->ctx->launches++;
   return cudaGetLastError();
 }

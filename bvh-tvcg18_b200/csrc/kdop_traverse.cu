@@ -85,111 +85,96 @@ __device__ __forceinline__ void ldg256(const float4* p, float4& x, float4& y) {
 __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(const volatile unsigned*)p; }
 __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
 
-// Overlap of the child pairs of one deque entry.  Side X is either a leaf
-// node (1 candidate: the node itself) or an internal node given by its first
-// child c (2 candidates: c, c + 1).  The records are fetched G float4 chunks
-// per round (all loads of a round in flight together); the next round is only
-// fetched while some child pair is still undecided.
-template <int K, int G>
-struct Expand {
+// Overlap of two single nodes by one lane (the root test of a mesh pair): both
+// records chunk by chunk; wa, wb get the records' word 0.
+template <int K>
+__device__ __forceinline__ bool node_overlap(const float4* __restrict__ nodes, uint32_t na, uint32_t nb,
+                                             uint32_t& wa, uint32_t& wb) {
   using L = NodeLayout<K>;
-  uint32_t idxA[2], idxB[2];  // node indices of the candidates
-  uint32_t stA[2], enA[2], stB[2], enB[2];
-  int na, nb;
-  unsigned sep;  // bit (2 i + k): child pair (i, k) separated (or absent)
-
-  __device__ __forceinline__ void chunk(int j, const float4& A0, const float4& A1, const float4& B0,
-                                        const float4& B1) {
-    if (2 * j < L::NS) {
-      // separated iff A.hi < B.lo || B.hi < A.lo
-      sep |= ((A0.y < B0.x) || (B0.y < A0.x)) ? 1u : 0u;
-      sep |= ((A0.y < B1.x) || (B1.y < A0.x)) ? 2u : 0u;
-      sep |= ((A1.y < B0.x) || (B0.y < A1.x)) ? 4u : 0u;
-      sep |= ((A1.y < B1.x) || (B1.y < A1.x)) ? 8u : 0u;
-    }
-    if (2 * j + 1 < L::NS) {
-      sep |= ((A0.w < B0.z) || (B0.w < A0.z)) ? 1u : 0u;
-      sep |= ((A0.w < B1.z) || (B1.w < A0.z)) ? 2u : 0u;
-      sep |= ((A1.w < B0.z) || (B0.w < A1.z)) ? 4u : 0u;
-      sep |= ((A1.w < B1.z) || (B1.w < A1.z)) ? 8u : 0u;
-    }
+  bool sep = false;
+  wa = wb = 0;
+#pragma unroll
+  for (int j = 0; j < L::NW; ++j) {
+    float4 A = __ldg(nodes + L::at(na, j)), B = __ldg(nodes + L::at(nb, j));
+    if (2 * j < L::NS) sep |= (A.y < B.x) || (B.y < A.x);
+    if (2 * j + 1 < L::NS) sep |= (A.w < B.z) || (B.w < A.z);
     if (j == L::TOPO_CHUNK) {
-      stA[0] = __float_as_uint(L::TOPO_ZW ? A0.z : A0.x);
-      enA[0] = __float_as_uint(L::TOPO_ZW ? A0.w : A0.y);
-      stA[1] = __float_as_uint(L::TOPO_ZW ? A1.z : A1.x);
-      enA[1] = __float_as_uint(L::TOPO_ZW ? A1.w : A1.y);
-      stB[0] = __float_as_uint(L::TOPO_ZW ? B0.z : B0.x);
-      enB[0] = __float_as_uint(L::TOPO_ZW ? B0.w : B0.y);
-      stB[1] = __float_as_uint(L::TOPO_ZW ? B1.z : B1.x);
-      enB[1] = __float_as_uint(L::TOPO_ZW ? B1.w : B1.y);
+      wa = L::word0(A);
+      wb = L::word0(B);
     }
   }
+  return !sep;
+}
 
-  __device__ __forceinline__ void run(const float4* __restrict__ nodes, uint32_t ea, uint32_t eb) {
-    na = (ea & LEAF_BIT) ? 1 : 2;
-    nb = (eb & LEAF_BIT) ? 1 : 2;
-    uint32_t a0 = ea & ~LEAF_BIT, b0 = eb & ~LEAF_BIT;
-    idxA[0] = a0;
-    idxA[1] = a0 + 1;
-    idxB[0] = b0;
-    idxB[1] = b0 + 1;
-    sep = 0;
-    if (na == 1) sep |= 0xC;  // pairs (1,0), (1,1)
-    if (nb == 1) sep |= 0xA;  // pairs (0,1), (1,1)
-    const float4* pa = nodes + (int64_t)a0 * L::NW;
-    const float4* pb = nodes + (int64_t)b0 * L::NW;
-    stA[0] = stA[1] = enA[0] = enA[1] = stB[0] = stB[1] = enB[0] = enB[1] = 0;
-    // Records of an even number of chunks start on 32-byte boundaries, so
-    // two chunks come in one 256-bit load (half the L1 wavefronts).
-    constexpr bool kWide = (L::NW % 2 == 0) && (G % 2 == 0);
+// Waiting warps from which on every deque with work donates (tail mode).
+constexpr int kTailWaiting = 64;
+
+// Warp total and exclusive prefix of per-lane counts below 2^BITS, one
+// ballot per bit.
+template <int BITS>
+__device__ __forceinline__ void warp_prefix(int v, unsigned lt_mask, int& total, int& excl) {
+  total = excl = 0;
 #pragma unroll
-    for (int j0 = 0; j0 < L::NW; j0 += G) {
-      if (sep == 0xF) break;
-      float4 A0[G], A1[G], B0[G], B1[G];
-      if (kWide) {
-#pragma unroll
-        for (int g = 0; g < G; g += 2) {
-          if (j0 + g < L::NW) {
-            ldg256(pa + j0 + g, A0[g], A0[g + 1]);
-            ldg256(pb + j0 + g, B0[g], B0[g + 1]);
-            A1[g] = A0[g];
-            A1[g + 1] = A0[g + 1];
-            B1[g] = B0[g];
-            B1[g + 1] = B0[g + 1];
-            if (na == 2) ldg256(pa + L::NW + j0 + g, A1[g], A1[g + 1]);
-            if (nb == 2) ldg256(pb + L::NW + j0 + g, B1[g], B1[g + 1]);
-          }
-        }
-      } else {
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-          if (j0 + g < L::NW) {
-            A0[g] = __ldg(pa + j0 + g);
-            B0[g] = __ldg(pb + j0 + g);
-            A1[g] = A0[g];
-            B1[g] = B0[g];
-            if (na == 2) A1[g] = __ldg(pa + L::NW + j0 + g);
-            if (nb == 2) B1[g] = __ldg(pb + L::NW + j0 + g);
-          }
-        }
-      }
-#pragma unroll
-      for (int g = 0; g < G; ++g)
-        if (j0 + g < L::NW) chunk(j0 + g, A0[g], A1[g], B0[g], B1[g]);
-    }
+  for (int k = 0; k < BITS; ++k) {
+    unsigned m = __ballot_sync(0xffffffffu, (v >> k) & 1);
+    total += __popc(m) << k;
+    excl += __popc(m & lt_mask) << k;
   }
+}
+
+// Tet of a leaf node (word 1 of its record).
+template <int K>
+__device__ __forceinline__ uint32_t leaf_tet(const float4* __restrict__ nodes, uint32_t w) {
+  using L = NodeLayout<K>;
+  return L::word1(__ldg(nodes + L::at(w & NODE_MASK, L::TOPO_CHUNK)));
+}
+
+// Lanes per deque entry: chunk pairs of a record over C chunks per lane,
+// rounded up to a power of two so that entries sit on aligned lane groups.
+template <int K, int C>
+struct Coop {
+  static constexpr int NW = NodeLayout<K>::NW;
+  static constexpr int Q0 = (NW + C - 1) / C;
+  static constexpr int Q = Q0 <= 1 ? 1 : Q0 <= 2 ? 2 : Q0 <= 4 ? 4 : 8;
+  static constexpr int E = 32 / Q;             // entries per sub-batch
+  static constexpr int PM = (4 + Q - 1) / Q;   // child pairs per lane
 };
 
-template <int K, int G>
+// Deque entries (X, Y, pair): X and Y overlap and their children are to be
+// tested.  A side with LEAF_BIT is the single node X & NODE_MASK (a leaf);
+// otherwise X is the first child of an internal node, whose children X, X + 1
+// form one twin record.  Word 0 of a child's record is its entry value.
+//
+// Cooperative expansion: Q lanes take one entry (E = 32 / Q entries per
+// sub-batch).  Lane q reads chunks j = q, q + Q, ... (C of them) of both
+// children of each side, one 256-bit load per chunk and side (twin records
+// interleave the siblings' chunks), so the lanes of an entry read whole
+// 128-byte lines (k = 14) and a warp-wide load touches E lines instead of 32.
+// The lane tests its slabs for the four child pairs; a butterfly OR over the
+// entry's lanes combines the verdicts; the lane holding the topology chunk
+// broadcasts the children's word 0; lane q then handles child pairs q, q + Q.
+// S sub-batches are loaded together per step, and one compaction per step
+// packs the pushes of all of them.
+template <int K, int C, int S>
 __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
+  using L = NodeLayout<K>;
+  using CP = Coop<K, C>;
+  constexpr int NW = L::NW;
+  constexpr int Q = CP::Q, E = CP::E, PM = CP::PM;
+  constexpr int SLOTS = PM * S;                     // pushes per lane per step
+  constexpr int TQ = L::TOPO_CHUNK % Q, TR = L::TOPO_CHUNK / Q;  // lane and round holding topology
+  constexpr int CBITS = SLOTS <= 1 ? 1 : SLOTS <= 3 ? 2 : 3;  // bits of a lane's push count
   extern __shared__ uint32_t smem[];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
+  const int ge = lane / Q, gq = lane % Q;  // entry and chunk lane of this lane
+  const unsigned lt_mask = (1u << lane) - 1u;
   const int CAP = a.stack_cap;
   const int MASK = CAP - 1;
-  uint32_t* sA = smem + (size_t)wib * 3 * CAP;
-  uint32_t* sB = sA + CAP;
-  uint32_t* sP = sB + CAP;
+  // this warp's deque: CAP entries of (A, B) words, then CAP pair indices
+  uint32_t* wbase = smem + (size_t)wib * 3 * CAP;
+  uint2* sAB = reinterpret_cast<uint2*>(wbase);
+  uint32_t* sP = wbase + 2 * CAP;
   TravCtl* ctl = a.ctl;
   const unsigned n_init = ctl->n_init;
   const unsigned pair_base = ctl->pair_base;
@@ -202,19 +187,21 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
   unsigned max_depth = 0;
   bool failed = false;
 
+  unsigned step = 0;
   for (;;) {
-    // per-lane results of this step
-    unsigned push_mask = 0, emit_mask = 0;
-    uint32_t pushA[4], pushB[4], emitA[4], emitB[4];
-    uint32_t pid = 0;
-
-    // queue counters for the donation check, read early so that their
-    // latency overlaps the node loads of this step
+    // Queue counters for the donation check, read early so that their
+    // latency overlaps the node loads of this step: every step while the
+    // deque is deep, every 8th step while it holds a little work (so that
+    // the traversal's tail, when most warps wait, is spread again).
     unsigned q_h = 0, q_t = 0;
-    if (lane == 0 && top - bot >= a.donate_min) {
+    ++step;
+    if (lane == 0 && (top - bot >= a.donate_min || (top - bot >= 2 && (step & 7u) == 0u))) {
       q_h = ld_volatile(&ctl->q_head);
       q_t = ld_volatile(&ctl->q_tail);
     }
+    // this step's pushes (entry words) and emitted leaf pairs (node words)
+    unsigned push_mask = 0, emit_mask = 0;
+    uint32_t pushA[SLOTS], pushB[SLOTS], slotP[SLOTS];
 
     if (top == bot) {
       // Work handed to the queue was counted before it was published, so the
@@ -235,7 +222,7 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
           if (lane < n) {
             // root test (kdop_tandem_traversal.h:164), then the traversal's own
             // test of the root pair (:42), both counted as the reference does.
-            pid = pair_base + base + lane;
+            uint32_t pid = pair_base + base + lane;
             if (a.order) pid = a.order[pid];
             uint2 mp = a.pairs[pid];
             uint32_t ra = NO_NODE, rb = NO_NODE;
@@ -246,23 +233,19 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
               atomicOr(&ctl->error, DEV_ERR_BAD_INDEX);
             }
             if (ra != NO_NODE && rb != NO_NODE) {
-              Expand<K, G> ex;
-              ex.run(a.nodes, ra | LEAF_BIT, rb | LEAF_BIT);
+              uint32_t wa, wb;
+              bool ov = node_overlap<K>(a.nodes, ra, rb, wa, wb);
               my_tests += 1;
-              if (!(ex.sep & 1u)) {
+              if (ov) {
                 my_tests += 1;
-                bool la = ex.stA[0] == ex.enA[0], lb = ex.stB[0] == ex.enB[0];
-                if (la && lb) {
+                pushA[0] = wa;
+                pushB[0] = wb;
+                slotP[0] = pid;
+                if (wa & wb & LEAF_BIT) {
                   my_lo += 1;
-                  if (!a.surface_filter || (a.surf[ex.stA[0]] && a.surf[ex.stB[0]])) {
-                    emit_mask = 1;
-                    emitA[0] = ex.stA[0];
-                    emitB[0] = ex.stB[0];
-                  }
+                  if (!a.surface_filter || (wa & wb & SURF_BIT)) emit_mask = 1;
                 } else {
                   push_mask = 1;
-                  pushA[0] = la ? (ra | LEAF_BIT) : ex.stA[0];
-                  pushB[0] = lb ? (rb | LEAF_BIT) : ex.stB[0];
                 }
               }
             }
@@ -281,12 +264,14 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
         unsigned long long t0 = global_ns();
         unsigned backoff = 64;
         int got = 0;
-        for (;;) {
+        for (unsigned it = 0;; ++it) {
           if (claim < a.q_cap && ld_volatile(&a.q_tags[claim]) != 0u) {
             got = 1;
             break;
           }
-          if (ld_volatile(&ctl->work) == 0) break;
+          // the end-of-work counter is polled by every waiting warp: every
+          // 4th round only, to keep its line free for the workers' atomics
+          if ((it & 3u) == 0u && ld_volatile(&ctl->work) == 0) break;
           if ((long long)(global_ns() - t0) > a.timeout_ns) {
             failed = true;
             break;
@@ -304,8 +289,7 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
         uint4 it = __ldcg(a.q_items + claim);
         if (lane == 0) {
           a.q_tags[claim] = 0u;
-          sA[top & MASK] = it.x;
-          sB[top & MASK] = it.y;
+          sAB[top & MASK] = make_uint2(it.x, it.y);
           sP[top & MASK] = it.z;
         }
         top += 1;
@@ -315,106 +299,162 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
         continue;
       }
     } else {
-      int n = min(32, top - bot);
+      const int n = min(E * S, top - bot);
       top -= n;
-      if (lane < n) {
-        int at = (top + lane) & MASK;
-        uint32_t ea = sA[at], eb = sB[at];
-        pid = sP[at];
-        Expand<K, G> ex;
-        ex.run(a.nodes, ea, eb);
-        my_tests += (unsigned long long)(ex.na * ex.nb);
+      uint2 eab[S];
+      uint32_t ep[S];
+      float4 A0[S][C], A1[S][C], B0[S][C], B1[S][C];
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          int i = c >> 1, k = c & 1;
-          if (ex.sep & (1u << c)) continue;
-          bool la = ex.stA[i] == ex.enA[i], lb = ex.stB[k] == ex.enB[k];
-          if (la && lb) {
-            my_lo += 1;
-            if (!a.surface_filter || (a.surf[ex.stA[i]] && a.surf[ex.stB[k]])) {
-              emit_mask |= 1u << c;
-              emitA[c] = ex.stA[i];
-              emitB[c] = ex.stB[k];
-            }
+      for (int b = 0; b < S; ++b) {
+        const int i = b * E + ge;
+        eab[b] = make_uint2(0u, 0u);
+        ep[b] = 0;
+        if (i < n) {
+          const int at = (top + i) & MASK;
+          eab[b] = sAB[at];
+          ep[b] = sP[at];
+        }
+        const int64_t ta = (int64_t)((eab[b].x & NODE_MASK) >> 1) * (2 * NW);
+        const int64_t tb = (int64_t)((eab[b].y & NODE_MASK) >> 1) * (2 * NW);
+#pragma unroll
+        for (int r = 0; r < C; ++r) {
+          const int j = gq + Q * r;
+          if (i < n && j < NW) {
+            ldg256(a.nodes + ta + 2 * j, A0[b][r], A1[b][r]);
+            ldg256(a.nodes + tb + 2 * j, B0[b][r], B1[b][r]);
           } else {
-            push_mask |= 1u << c;
-            pushA[c] = la ? (ex.idxA[i] | LEAF_BIT) : ex.stA[i];
-            pushB[c] = lb ? (ex.idxB[k] | LEAF_BIT) : ex.stB[k];
+            A0[b][r] = A1[b][r] = B0[b][r] = B1[b][r] = make_float4(0.f, 0.f, 0.f, 0.f);
           }
         }
       }
-      __syncwarp();
-    }
-
-    // ---- compaction: one warp prefix sum of (pushes, emits) ----
-    int np = __popc(push_mask), ne = __popc(emit_mask);
-    int v = np | (ne << 16);
-    int incl = v;
+      __syncwarp();  // entries read before this step's pushes overwrite them
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      int y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
+      for (int b = 0; b < S; ++b) {
+        const bool valid = b * E + ge < n;
+        const uint32_t xa = eab[b].x, xb = eab[b].y;
+        const bool singleA = (xa & LEAF_BIT) != 0, singleB = (xb & LEAF_BIT) != 0;
+        // separation of child pairs (0,0), (0,1), (1,0), (1,1); absent pairs
+        // of a single side count as separated
+        bool s0 = false, s1 = singleB, s2 = singleA, s3 = singleA || singleB;
+        uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+#pragma unroll
+        for (int r = 0; r < C; ++r) {
+          const int j = gq + Q * r;
+          float4 a0 = A0[b][r], a1 = A1[b][r], b0 = B0[b][r], b1 = B1[b][r];
+          if (singleA && (xa & 1u)) a0 = a1;
+          if (singleB && (xb & 1u)) b0 = b1;
+          if (2 * j < L::NS) {
+            s0 = s0 || (a0.y < b0.x) || (b0.y < a0.x);
+            s1 = s1 || (a0.y < b1.x) || (b1.y < a0.x);
+            s2 = s2 || (a1.y < b0.x) || (b0.y < a1.x);
+            s3 = s3 || (a1.y < b1.x) || (b1.y < a1.x);
+          }
+          if (2 * j + 1 < L::NS) {
+            s0 = s0 || (a0.w < b0.z) || (b0.w < a0.z);
+            s1 = s1 || (a0.w < b1.z) || (b1.w < a0.z);
+            s2 = s2 || (a1.w < b0.z) || (b0.w < a1.z);
+            s3 = s3 || (a1.w < b1.z) || (b1.w < a1.z);
+          }
+          if (r == TR) {
+            t0 = L::word0(a0);
+            t1 = L::word0(a1);
+            t2 = L::word0(b0);
+            t3 = L::word0(b1);
+          }
+        }
+        unsigned sep = (s0 ? 1u : 0u) | (s1 ? 2u : 0u) | (s2 ? 4u : 0u) | (s3 ? 8u : 0u);
+#pragma unroll
+        for (int o = 1; o < Q; o <<= 1) sep |= __shfl_xor_sync(0xffffffffu, sep, o);
+        // word 0 of the four children, from the lane holding the topology chunk
+        const int src = ge * Q + TQ;
+        const uint32_t wA0 = __shfl_sync(0xffffffffu, t0, src);
+        const uint32_t wA1 = __shfl_sync(0xffffffffu, t1, src);
+        const uint32_t wB0 = __shfl_sync(0xffffffffu, t2, src);
+        const uint32_t wB1 = __shfl_sync(0xffffffffu, t3, src);
+        if (valid) {
+          if (gq == 0) my_tests += (unsigned long long)((singleA ? 1 : 2) * (singleB ? 1 : 2));
+#pragma unroll
+          for (int r = 0; r < PM; ++r) {
+            const int c = gq + Q * r;
+            if (c >= 4 || (sep & (1u << c))) continue;
+            const uint32_t wa = (c >> 1) ? wA1 : wA0, wb = (c & 1) ? wB1 : wB0;
+            const int k = b * PM + r;
+            pushA[k] = wa;
+            pushB[k] = wb;
+            slotP[k] = ep[b];
+            if (wa & wb & LEAF_BIT) {
+              my_lo += 1;
+              if (!a.surface_filter || (wa & wb & SURF_BIT)) emit_mask |= 1u << k;
+            } else {
+              push_mask |= 1u << k;
+            }
+          }
+        }
+      }
     }
-    int tot = __shfl_sync(0xffffffffu, incl, 31);
-    int excl = incl - v;
-    int tot_p = tot & 0xFFFF, tot_e = tot >> 16;
-    int off_p = excl & 0xFFFF, off_e = excl >> 16;
 
-    if (tot_e) {
+    // ---- emits (rare): leaf pairs to candidate rows, one atomic per warp ----
+    if (__any_sync(0xffffffffu, emit_mask != 0u)) {
+      int tot_e = 0, off_e = 0;
+      warp_prefix<CBITS>(__popc(emit_mask), lt_mask, tot_e, off_e);
       unsigned base = 0;
       if (lane == 0) base = atomicAdd(&ctl->n_cand, (unsigned)tot_e);
       base = __shfl_sync(0xffffffffu, base, 0) + (unsigned)off_e;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (emit_mask & (1u << c)) {
+      for (int k = 0; k < SLOTS; ++k) {
+        if (emit_mask & (1u << k)) {
           if (base < a.cand_cap) {
-            a.candA[base] = emitA[c];
-            a.candB[base] = emitB[c];
-            a.candP[base] = pid;
+            a.candA[base] = leaf_tet<K>(a.nodes, pushA[k]);
+            a.candB[base] = leaf_tet<K>(a.nodes, pushB[k]);
+            a.candP[base] = slotP[k];
           }
           ++base;
         }
       }
     }
-    if (tot_p) {
-      if (top - bot + tot_p <= CAP) {
-        int at = top + off_p;
+    // ---- pushes: ballot prefix sum, then deque (or the global queue) ----
+    {
+      int tot_p = 0, off_p = 0;
+      warp_prefix<CBITS>(__popc(push_mask), lt_mask, tot_p, off_p);
+      if (tot_p) {
+        if (top - bot + tot_p <= CAP) {
+          int at = top + off_p;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (push_mask & (1u << c)) {
-            sA[at & MASK] = pushA[c];
-            sB[at & MASK] = pushB[c];
-            sP[at & MASK] = pid;
-            ++at;
+          for (int k = 0; k < SLOTS; ++k) {
+            if (push_mask & (1u << k)) {
+              sAB[at & MASK] = make_uint2(pushA[k], pushB[k]);
+              sP[at & MASK] = slotP[k];
+              ++at;
+            }
           }
-        }
-        top += tot_p;
-      } else {
-        // deque full: the new entries go to the global queue
-        unsigned t0 = 0;
-        if (lane == 0) t0 = atomicAdd(&ctl->q_tail, (unsigned)tot_p);
-        t0 = __shfl_sync(0xffffffffu, t0, 0);
-        int room = (int)min((unsigned long long)tot_p,
-                            (t0 < a.q_cap) ? (unsigned long long)(a.q_cap - t0) : 0ull);
-        if (room < tot_p && lane == 0) atomicOr(&ctl->error, DEV_ERR_QUEUE_FULL);
-        if (room > 0 && lane == 0) atomicAdd(&ctl->work, room);
-        __syncwarp();
-        unsigned slot = t0 + (unsigned)off_p;
+          top += tot_p;
+        } else {
+          // deque full: the new entries go to the global queue
+          unsigned t0 = 0;
+          if (lane == 0) t0 = atomicAdd(&ctl->q_tail, (unsigned)tot_p);
+          t0 = __shfl_sync(0xffffffffu, t0, 0);
+          int room = (int)min((unsigned long long)tot_p,
+                              (t0 < a.q_cap) ? (unsigned long long)(a.q_cap - t0) : 0ull);
+          if (room < tot_p && lane == 0) atomicOr(&ctl->error, DEV_ERR_QUEUE_FULL);
+          if (room > 0 && lane == 0) atomicAdd(&ctl->work, room);
+          __syncwarp();
+          unsigned slot = t0 + (unsigned)off_p;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (push_mask & (1u << c)) {
-            if (slot < t0 + (unsigned)room) a.q_items[slot] = make_uint4(pushA[c], pushB[c], pid, 0u);
-            ++slot;
+          for (int k = 0; k < SLOTS; ++k) {
+            if (push_mask & (1u << k)) {
+              if (slot < t0 + (unsigned)room) a.q_items[slot] = make_uint4(pushA[k], pushB[k], slotP[k], 0u);
+              ++slot;
+            }
           }
-        }
-        __threadfence();
-        __syncwarp();
-        slot = t0 + (unsigned)off_p;
+          __threadfence();
+          __syncwarp();
+          slot = t0 + (unsigned)off_p;
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          if (push_mask & (1u << c)) {
-            if (slot < t0 + (unsigned)room) atomicExch(&a.q_tags[slot], 1u);
-            ++slot;
+          for (int k = 0; k < SLOTS; ++k) {
+            if (push_mask & (1u << k)) {
+              if (slot < t0 + (unsigned)room) atomicExch(&a.q_tags[slot], 1u);
+              ++slot;
+            }
           }
         }
       }
@@ -423,11 +463,13 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
     if ((unsigned)depth > max_depth) max_depth = (unsigned)depth;
 
     // ---- donation: give the oldest entries to waiting warps ----
-    if (depth >= a.donate_min) {
+    // A deep deque gives to any waiting warp; while many warps wait (the
+    // tail of the traversal) any deque with two or more entries gives half.
+    if (depth >= 2) {
       int waiting = 0;
-      if (lane == 0) waiting = (q_h > q_t) ? (int)min(q_h - q_t, 32u) : 0;
+      if (lane == 0) waiting = (q_h > q_t) ? (int)min(q_h - q_t, 1024u) : 0;
       waiting = __shfl_sync(0xffffffffu, waiting, 0);
-      int d = min(waiting, depth / 2);
+      int d = (depth >= a.donate_min || waiting >= kTailWaiting) ? min(min(waiting, 32), depth / 2) : 0;
       if (d > 0) {
         unsigned t0 = 0;
         if (lane == 0) t0 = atomicAdd(&ctl->q_tail, (unsigned)d);
@@ -438,7 +480,8 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
         __syncwarp();
         if (lane < room) {
           int at = (bot + lane) & MASK;
-          a.q_items[t0 + lane] = make_uint4(sA[at], sB[at], sP[at], 0u);
+          uint2 ab = sAB[at];
+          a.q_items[t0 + lane] = make_uint4(ab.x, ab.y, sP[at], 0u);
         }
         __threadfence();
         __syncwarp();
@@ -489,11 +532,11 @@ size_t traverse_smem_bytes(int block_warps, int stack_cap) {
 
 template <int K>
 static cudaError_t prepare_k(size_t smem) {
-  cudaError_t e = cudaFuncSetAttribute(traverse_kernel<K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaFuncSetAttribute(traverse_kernel<K, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(traverse_kernel<K, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(traverse_kernel<K, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(traverse_kernel<K, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = cudaFuncSetAttribute(traverse_kernel<K, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return e;
 }
 
@@ -510,7 +553,7 @@ cudaError_t traverse_prepare(int K, size_t smem) {
   return cudaErrorInvalidValue;
 }
 
-template <int K, int G>
+template <int K, int C, int S>
 static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffers& b, const TravParams& p,
                                  int plain) {
   cudaStream_t st = s->ctx->stream;
@@ -518,11 +561,11 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
   size_t smem = traverse_smem_bytes(p.block_warps, p.stack_cap);
   cudaError_t e = prepare_k<K>(smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(traverse_kernel<K, G>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  e = cudaFuncSetAttribute(traverse_kernel<K, C, S>, cudaFuncAttributePreferredSharedMemoryCarveout,
                            p.smem_carveout > 0 ? p.smem_carveout : -1);
   if (e != cudaSuccess) return e;
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_kernel<K, G>, threads, smem);
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, traverse_kernel<K, C, S>, threads, smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) return cudaErrorInvalidConfiguration;
   unsigned grid = (unsigned)(per_sm * s->ctx->sm_count);
@@ -553,14 +596,14 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
     for (int64_t off = 0; off < n_pairs || off == 0; off += wave) {
       int64_t n = std::min<int64_t>(wave, n_pairs - off);
       trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)std::max<int64_t>(n, 0), (unsigned)off, off == 0);
-      traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
+      traverse_kernel<K, C, S><<<grid, threads, smem, st>>>(a);
       s->ctx->launches += 2;
       if (n_pairs == 0) break;
     }
   } else {
     for (int64_t i = 0; i < n_pairs; ++i) {
       trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 1u, (unsigned)i, i == 0 ? 1 : 0);
-      traverse_kernel<K, G><<<grid, threads, smem, st>>>(a);
+      traverse_kernel<K, C, S><<<grid, threads, smem, st>>>(a);
       s->ctx->launches += 2;
     }
     if (n_pairs == 0) {
@@ -574,10 +617,13 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
 template <int K>
 static cudaError_t traverse_group(kdop_scene* s, int64_t n_pairs, const TravBuffers& b, const TravParams& p,
                                   int plain) {
+  // load_group: 1 = one chunk pair per lane, one sub-batch per step;
+  // 2 = two sub-batches per step; 4 = two chunk pairs per lane (half the
+  // lanes per entry, twice the entries per sub-batch)
   switch (p.load_group) {
-    case 1: return traverse_impl<K, 1>(s, n_pairs, b, p, plain);
-    case 4: return traverse_impl<K, 4>(s, n_pairs, b, p, plain);
-    default: return traverse_impl<K, 2>(s, n_pairs, b, p, plain);
+    case 1: return traverse_impl<K, 1, 1>(s, n_pairs, b, p, plain);
+    case 4: return traverse_impl<K, 2, 1>(s, n_pairs, b, p, plain);
+    default: return traverse_impl<K, 1, 2>(s, n_pairs, b, p, plain);
   }
 }
 
@@ -618,7 +664,7 @@ namespace kdop {
 namespace {
 
 constexpr int64_t kStaticQueueEntries = 65536;
-constexpr size_t kStaticCtlBytes = 256;
+constexpr size_t kStaticCtlBytes = 1024;
 constexpr size_t kStaticTagBytes = (size_t)kStaticQueueEntries * sizeof(uint32_t);
 constexpr size_t kStaticScratchBytes = kStaticCtlBytes + kStaticTagBytes + (size_t)kStaticQueueEntries * sizeof(uint4);
 static_assert(sizeof(TravCtl) <= kStaticCtlBytes, "control block does not fit");

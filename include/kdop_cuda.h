@@ -153,7 +153,9 @@ typedef struct {
   int32_t init_chunk;     /* root pairs taken per queue claim (0: default) */
   int32_t donate_min;     /* stack size from which a warp gives work to idle warps (0: default) */
   int32_t timeout_ms;     /* bound of every device-side wait (0: 5000) */
-  int32_t load_group;     /* float4 chunks of a node record fetched per round: 1, 2 or 4 (0: default) */
+  int32_t load_group;     /* expansion shape (0: default 4): 1 = one 32-byte chunk pair per lane
+                             and one batch of entries per step, 2 = two batches per step,
+                             4 = two chunk pairs per lane (half the lanes per entry) */
   int32_t wave_pairs;     /* pairs per persistent launch, largest first (0: all pairs in one launch) */
   int32_t smem_carveout;  /* shared-memory share of the L1/shared array in percent (0: driver choice) */
 } kdop_traverse_opts;
