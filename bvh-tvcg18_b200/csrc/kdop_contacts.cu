@@ -13,10 +13,14 @@
 //      all candidates, points projected on the mid plane, near-duplicates
 //      (max-norm < 10 FLT_EPSILON) dropped, reported in order (:622-681).
 //
-// One warp handles one candidate tet pair: lanes evaluate the 44 SAT axes,
-// the 16 face pairs and the 56 contact candidates in parallel; ballots keep
-// the reference's candidate order, so the reported rows and every value equal
-// the reference's FP32 results.
+// Two passes.  A thread per candidate tet pair first runs steps 1 and 2 up
+// to the first separating axis or the first admissible face pair (almost all
+// leaf pairs of a deep overlap stop there: no contact) and lists the pairs
+// that go on.  Then one warp handles each listed pair: lanes evaluate the 44
+// SAT axes, the 16 face pairs and the 56 contact candidates in parallel;
+// ballots keep the reference's candidate order, so the reported rows and
+// every value equal the reference's FP32 results.  Both passes evaluate the
+// same functions on the same inputs, so their decisions agree.
 #include "kdop_device.cuh"
 
 namespace kdop {
@@ -141,6 +145,7 @@ struct ContactArgs {
   const uint32_t* candA;
   const uint32_t* candB;
   const uint32_t* candP;
+  uint32_t* surv;  // candidates past the pre-filter (n_surv of them)
   unsigned cand_cap;
   const uint4* __restrict__ tets;
   const uint8_t* __restrict__ surf;
@@ -153,15 +158,80 @@ struct ContactArgs {
 
 constexpr int WARPS_PER_BLOCK_C = 8;
 
+// Face pair (fa, fb) admissible as the most opposing pair (…_tetrahedron_
+// tetrahedron.h:465-533): both boundary faces, opposing unit normals, and
+// each tet's opposite vertex not behind the other's face plane.
+__device__ __forceinline__ bool face_pair_ok(int fa, int fb, uint32_t sa, uint32_t sb, const UPlane* PA,
+                                             const UPlane* PB, const f3* A, const f3* B, float& test, f3& nA) {
+  if (!(((sa >> fa) & 1u) && ((sb >> fb) & 1u))) return false;
+  const UPlane& pa = PA[fa];
+  const UPlane& pb = PB[fb];
+  nA = unit3(pa.n);
+  f3 nB = unit3(pb.n);
+  float t = dot3(nA, nB);
+  if (!(t < 0.f)) return false;
+  float tA = dot3(pa.n, sub3(B[fb], pa.p));
+  float tB = dot3(pb.n, sub3(A[fa], pb.p));
+  if ((tA < 0.f) || (tB < 0.f)) return false;
+  test = t;
+  return true;
+}
+
+// Pass 1: thread per candidate.  A pair that fails the SAT test or has no
+// admissible face pair gets its empty record here; the others are listed.
+__global__ void __launch_bounds__(256) contacts_filter_kernel(ContactArgs a) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const unsigned n_cand = min(*(volatile unsigned*)&a.ctl->n_cand, a.cand_cap);
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_cand; base += stride) {
+    const unsigned ci = base + lane;
+    bool keep = false;
+    if (ci < n_cand) {
+      uint32_t ta = a.candA[ci], tb = a.candB[ci];
+      uint32_t sa = a.surf[ta], sb = a.surf[tb];
+      if (sa != 0u && sb != 0u) {
+        uint4 qa = __ldg(a.tets + ta), qb = __ldg(a.tets + tb);
+        f3 A[4] = {world_vertex(a.vs, qa.x), world_vertex(a.vs, qa.y), world_vertex(a.vs, qa.z),
+                   world_vertex(a.vs, qa.w)};
+        f3 B[4] = {world_vertex(a.vs, qb.x), world_vertex(a.vs, qb.y), world_vertex(a.vs, qb.z),
+                   world_vertex(a.vs, qb.w)};
+        bool sep = false;
+        for (int t = 0; t < 44 && !sep; ++t) sep = sat_test(t, A, B);
+        if (!sep) {
+          UPlane PA[4], PB[4];
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            PA[f] = unscaled_plane(A[c_face[f][0]], A[c_face[f][1]], A[c_face[f][2]]);
+            PB[f] = unscaled_plane(B[c_face[f][0]], B[c_face[f][1]], B[c_face[f][2]]);
+          }
+          float test;
+          f3 nA;
+          for (int l = 0; l < 16 && !keep; ++l) keep = face_pair_ok(l >> 2, l & 3, sa, sb, PA, PB, A, B, test, nA);
+        }
+      }
+      if (!keep) a.rec[ci] = make_int4(-1, -1, 0, 0);
+    }
+    unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (m) {
+      unsigned at = 0;
+      if (lane == 0) at = atomicAdd(&a.ctl->n_surv, (unsigned)__popc(m));
+      at = __shfl_sync(0xffffffffu, at, 0);
+      if (keep) a.surv[at + __popc(m & lt_mask)] = ci;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK_C) contacts_kernel(ContactArgs a) {
   __shared__ float s_pts[WARPS_PER_BLOCK_C][56][3];
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const unsigned lt_mask = (1u << lane) - 1u;
-  unsigned n_cand = min(*(volatile unsigned*)&a.ctl->n_cand, a.cand_cap);
+  unsigned n_surv = *(volatile unsigned*)&a.ctl->n_surv;
   unsigned warp = blockIdx.x * WARPS_PER_BLOCK_C + wib;
   unsigned n_warps = gridDim.x * WARPS_PER_BLOCK_C;
-  for (unsigned ci = warp; ci < n_cand; ci += n_warps) {
+  for (unsigned k = warp; k < n_surv; k += n_warps) {
+    const unsigned ci = a.surv[k];
     uint32_t ta = a.candA[ci], tb = a.candB[ci];
     int4 record = make_int4(-1, -1, 0, 0);
     uint32_t sa = a.surf[ta], sb = a.surf[tb];
@@ -206,24 +276,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK_C) contacts_kernel(Contac
       float test = 3.0e38f;
       bool good = false;
       f3 nA = mk3(0.f, 0.f, 0.f);
-      if (lane < 16) {
-        int fa = lane >> 2, fb = lane & 3;
-        if (((sa >> fa) & 1u) && ((sb >> fb) & 1u)) {
-          const UPlane& pa = PA[fa];
-          const UPlane& pb = PB[fb];
-          nA = unit3(pa.n);
-          f3 nB = unit3(pb.n);
-          float t = dot3(nA, nB);
-          if (t < 0.f) {
-            float tA = dot3(pa.n, sub3(B[fb], pa.p));
-            float tB = dot3(pb.n, sub3(A[fa], pb.p));
-            if (!(tA < 0.f) && !(tB < 0.f)) {
-              test = t;
-              good = true;
-            }
-          }
-        }
-      }
+      if (lane < 16) good = face_pair_ok(lane >> 2, lane & 3, sa, sb, PA, PB, A, B, test, nA);
       // first (a, b) in loop order with the smallest value
       float bv = good ? test : 3.0e38f;
       int bl = good ? lane : 64;
@@ -477,7 +530,10 @@ __global__ void __launch_bounds__(128) adjoint_kernel(AdjointArgs a) {
 }
 
 __global__ void contacts_reset_kernel(TravCtl* c) {
-  if (threadIdx.x == 0) c->n_contacts = 0;
+  if (threadIdx.x == 0) {
+    c->n_contacts = 0;
+    c->n_surv = 0;
+  }
 }
 
 static VertexSource vsrc(kdop_scene* s) {
@@ -498,6 +554,7 @@ cudaError_t launch_contacts(kdop_scene* s) {
   a.candA = s->cand;
   a.candB = s->cand + s->cand_cap;
   a.candP = s->cand + 2 * s->cand_cap;
+  a.surv = s->cand + 3 * s->cand_cap;
   a.cand_cap = (unsigned)s->cand_cap;
   a.tets = s->tets;
   a.surf = s->surf;
@@ -508,8 +565,9 @@ cudaError_t launch_contacts(kdop_scene* s) {
   a.ctl = s->ctl;
   contacts_reset_kernel<<<1, 32, 0, s->ctx->stream>>>(s->ctl);
   unsigned grid = (unsigned)s->ctx->sm_count * 8u;
+  contacts_filter_kernel<<<grid, 256, 0, s->ctx->stream>>>(a);
   contacts_kernel<<<grid, 32 * WARPS_PER_BLOCK_C, 0, s->ctx->stream>>>(a);
-  s->ctx->launches += 2;
+  s->ctx->launches += 3;
   return cudaGetLastError();
 }
 

@@ -32,7 +32,8 @@ struct TravCtl {
   unsigned int n_init;               // root pairs in this launch
   unsigned int pair_base;            // pair index of the first root pair
   unsigned int max_stack;            // deepest warp stack seen
-  unsigned int pad0[23];
+  unsigned int n_surv;               // candidates past the contact pre-filter
+  unsigned int pad0[22];
   unsigned int n_cand;               // candidates emitted (may exceed capacity)
   unsigned int pad1[31];
   unsigned int init_head;            // root pairs claimed
@@ -111,7 +112,7 @@ struct kdop_scene {
   uint2* pairs = nullptr;
   uint32_t* pair_order = nullptr;  // pair indices by decreasing size (tets of A + tets of B)
   int64_t pairs_cap = 0;
-  uint32_t* cand = nullptr;  // 3 * cand_cap: A tets | B tets | pair ids
+  uint32_t* cand = nullptr;  // 4 * cand_cap: A tets | B tets | pair ids | pre-filter survivors
   int64_t cand_cap = 0;
   kdop_contact* contacts = nullptr;
   int4* records = nullptr;  // per candidate: faces, candidate codes, count, first contact

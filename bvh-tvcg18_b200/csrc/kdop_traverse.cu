@@ -333,16 +333,18 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
         const bool valid = b * E + ge < n;
         const uint32_t xa = eab[b].x, xb = eab[b].y;
         const bool singleA = (xa & LEAF_BIT) != 0, singleB = (xb & LEAF_BIT) != 0;
-        // separation of child pairs (0,0), (0,1), (1,0), (1,1); absent pairs
-        // of a single side count as separated
-        bool s0 = false, s1 = singleB, s2 = singleA, s3 = singleA || singleB;
+        // Separation of child pairs (0,0), (0,1), (1,0), (1,1).  A single
+        // side is the node itself, which is side (x & 1) of the twin just
+        // loaded: the pairs with the other side of that twin are absent and
+        // count as separated.
+        const bool noA0 = singleA && (xa & 1u), noA1 = singleA && !(xa & 1u);
+        const bool noB0 = singleB && (xb & 1u), noB1 = singleB && !(xb & 1u);
+        bool s0 = noA0 || noB0, s1 = noA0 || noB1, s2 = noA1 || noB0, s3 = noA1 || noB1;
         uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0;
 #pragma unroll
         for (int r = 0; r < C; ++r) {
           const int j = gq + Q * r;
-          float4 a0 = A0[b][r], a1 = A1[b][r], b0 = B0[b][r], b1 = B1[b][r];
-          if (singleA && (xa & 1u)) a0 = a1;
-          if (singleB && (xb & 1u)) b0 = b1;
+          const float4 a0 = A0[b][r], a1 = A1[b][r], b0 = B0[b][r], b1 = B1[b][r];
           if (2 * j < L::NS) {
             s0 = s0 || (a0.y < b0.x) || (b0.y < a0.x);
             s1 = s1 || (a0.y < b1.x) || (b1.y < a0.x);
