@@ -636,7 +636,7 @@ int kdop_resolve_traverse_opts(const kdop_scene* s, const kdop_traverse_opts* o,
   if (p.smem_carveout > 100) return KDOP_ERR_INVALID;
   if (p.block_warps > 16 || (p.stack_cap & (p.stack_cap - 1)) || p.stack_cap < 64 || p.init_chunk > 32)
     return KDOP_ERR_INVALID;
-  if (p.load_group != 1 && p.load_group != 2 && p.load_group != 4) return KDOP_ERR_INVALID;
+  if (p.load_group != 1 && p.load_group != 2 && p.load_group != 4 && p.load_group != 8) return KDOP_ERR_INVALID;
   if (kdop::traverse_smem_bytes(p.block_warps, p.stack_cap) > s->ctx->smem_optin) return KDOP_ERR_INVALID;
   return KDOP_OK;
 }
@@ -985,7 +985,7 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   kdop_resolve_traverse_opts(s, &d, cur, mode);
   float best_ms = time_config(s, n_pairs, cur, repeats, e0, e1);
   if (best_ms < 0.f) best_ms = 1e30f;
-  const std::vector<int> warps = {4, 8, 16}, caps = {128, 256, 512, 1024}, groups = {1, 2, 4},
+  const std::vector<int> warps = {4, 8, 16}, caps = {128, 256, 512, 1024}, groups = {1, 2, 4, 8},
                          donate = {32, 64, 128, 256}, waves = {0, 16, 64, 128}, carve = {0, 25, 50, 100},
                          chunk = {1, 4};
   for (int sweep = 0; sweep < 2; ++sweep) {

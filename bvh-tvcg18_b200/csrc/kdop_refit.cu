@@ -8,11 +8,11 @@
 // (cl/kernels/kdop_cl_refit_tree.cl:17-168).
 //
 // Here the forest is stored level by level, so one launch refits one level of
-// every tree at once, deepest level first.  Thread t writes float4 slot t of
-// the level's twin records (chunk j of node n at slot 2 NW (n / 2) + 2 j +
-// n % 2): consecutive threads write consecutive 16-byte words (fully coalesced
-// stores), and an internal node reads chunk j of its two children, the twin
-// record below it, as one 32-byte load.  Leaves transform their vertices on the fly when the scene is in
+// every tree at once, deepest level first, one thread per node: a leaf poses
+// its four vertices once and projects them on all K/2 directions; an internal
+// node reads its children's twin record (2 NW consecutive float4, independent
+// loads in flight together).  Two sibling threads write the interleaved
+// chunks of one twin, so every store instruction fills whole 32-byte sectors.  Leaves transform their vertices on the fly when the scene is in
 // pose or deform mode (narrow_update_kdop_bvh.h:154-165 fused into the leaf
 // pass, so no world-vertex array is written).  The upper levels, too small to
 // fill the GPU, are refitted by one block that walks them with block barriers.
@@ -20,97 +20,84 @@
 
 namespace kdop {
 
-template <int K>
-__device__ __forceinline__ float4 refit_chunk(const float4* nodes, int64_t node, int j, const uint4* __restrict__ tets,
-                                              const VertexSource& vs, const DirTable& dt, bool use_ldg) {
+// The record of one node: a leaf projects its tet's four (posed) vertices on
+// the K/2 directions (make_dop), an internal node takes the union of its two
+// children chunk by chunk (make_union); the topology words are kept.  Chunk
+// j of both children is one aligned 32-byte word of their twin record.
+template <int K, bool LDG>
+__device__ __forceinline__ void refit_node(float4* nodes, int64_t node, const uint4* __restrict__ tets,
+                                           const VertexSource& vs, const DirTable& dt) {
   using L = NodeLayout<K>;
-  float4 tc = use_ldg ? __ldg(nodes + L::at(node, L::TOPO_CHUNK)) : nodes[L::at(node, L::TOPO_CHUNK)];
+  const float4 tc = LDG ? __ldg(nodes + L::at(node, L::TOPO_CHUNK)) : nodes[L::at(node, L::TOPO_CHUNK)];
   const uint32_t w0 = L::word0(tc), w1 = L::word1(tc);
-  float w[4];
+  float w[4 * L::NW];
+#pragma unroll
+  for (int k = 0; k < 4 * L::NW; ++k) w[k] = 0.f;
   if (w0 & LEAF_BIT) {
-    uint4 t = __ldg(tets + w1);
-    f3 p[4] = {world_vertex(vs, t.x), world_vertex(vs, t.y), world_vertex(vs, t.z), world_vertex(vs, t.w)};
+    const uint4 t = __ldg(tets + w1);
+    const f3 p[4] = {world_vertex(vs, t.x), world_vertex(vs, t.y), world_vertex(vs, t.z), world_vertex(vs, t.w)};
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      int s = 2 * j + h;
-      if (s < L::NS) {
-        f3 d = mk3(dt.d[s][0], dt.d[s][1], dt.d[s][2]);
-        float lo = 3.40282346638528859812e+38f, hi = -3.40282346638528859812e+38f;
+    for (int s = 0; s < L::NS; ++s) {
+      const f3 d = mk3(dt.d[s][0], dt.d[s][1], dt.d[s][2]);
+      float lo = 3.40282346638528859812e+38f, hi = -3.40282346638528859812e+38f;
 #pragma unroll
-        for (int v = 0; v < 4; ++v) {
-          float pr = dot3(d, p[v]);
-          lo = smin(lo, pr);
-          hi = smax(hi, pr);
-        }
-        w[2 * h] = lo;
-        w[2 * h + 1] = hi;
-      } else {
-        w[2 * h] = 0.f;
-        w[2 * h + 1] = 0.f;
+      for (int v = 0; v < 4; ++v) {
+        const float pr = dot3(d, p[v]);
+        lo = smin(lo, pr);
+        hi = smax(hi, pr);
       }
+      w[2 * s] = lo;
+      w[2 * s + 1] = hi;
     }
   } else {
-    // chunk j of the children w0, w0 + 1: one aligned 32-byte word of their twin
-    float4 a, b;
-    if (use_ldg) {
-      a = __ldg(nodes + L::at(w0, j));
-      b = __ldg(nodes + L::at(w0, j) + 1);
-    } else {
-      a = nodes[L::at(w0, j)];
-      b = nodes[L::at(w0, j) + 1];
-    }
-    // lo: min(A.lo, B.lo) = (B < A) ? B : A ; hi: max(A.hi, B.hi) = (A < B) ? B : A
-    w[0] = smin(a.x, b.x);
-    w[1] = smax(a.y, b.y);
-    w[2] = smin(a.z, b.z);
-    w[3] = smax(a.w, b.w);
-    if (2 * j + 1 >= L::NS) {
-      w[2] = 0.f;
-      w[3] = 0.f;
-    }
-    if (2 * j >= L::NS) {
-      w[0] = 0.f;
-      w[1] = 0.f;
-    }
-  }
-  if (j == L::TOPO_CHUNK) {
-    if (L::TOPO_ZW) {
-      w[2] = tc.z;
-      w[3] = tc.w;
-    } else {
-      w[0] = tc.x;
-      w[1] = tc.y;
+    const float4* c = nodes + L::at(w0, 0);  // chunk 0 of child w0; child w0 + 1 follows each chunk
+#pragma unroll
+    for (int j = 0; j < L::NW; ++j) {
+      float4 a, b;
+      if (LDG) {
+        a = __ldg(c + 2 * j);
+        b = __ldg(c + 2 * j + 1);
+      } else {
+        a = c[2 * j];
+        b = c[2 * j + 1];
+      }
+      // lo: min(A.lo, B.lo) = (B < A) ? B : A ; hi: max(A.hi, B.hi) = (A < B) ? B : A
+      if (2 * j < L::NS) {
+        w[4 * j] = smin(a.x, b.x);
+        w[4 * j + 1] = smax(a.y, b.y);
+      }
+      if (2 * j + 1 < L::NS) {
+        w[4 * j + 2] = smin(a.z, b.z);
+        w[4 * j + 3] = smax(a.w, b.w);
+      }
     }
   }
-  return make_float4(w[0], w[1], w[2], w[3]);
+  w[L::TOPO_ZW ? 4 * L::TOPO_CHUNK + 2 : 4 * L::TOPO_CHUNK] = __uint_as_float(w0);
+  w[L::TOPO_ZW ? 4 * L::TOPO_CHUNK + 3 : 4 * L::TOPO_CHUNK + 1] = __uint_as_float(w1);
+#pragma unroll
+  for (int j = 0; j < L::NW; ++j)
+    nodes[L::at(node, j)] = make_float4(w[4 * j], w[4 * j + 1], w[4 * j + 2], w[4 * j + 3]);
 }
 
+// One level of every tree, thread per node.
 template <int K>
 __global__ void __launch_bounds__(256) refit_level_kernel(float4* nodes, int64_t begin, int64_t count,
                                                           const uint4* __restrict__ tets, VertexSource vs,
                                                           DirTable dt) {
-  using L = NodeLayout<K>;
   int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= count * L::NW) return;
-  int64_t f = begin * L::NW + t;  // float4 slot (begin and count are even)
-  int64_t node = 2 * (f / (2 * L::NW)) + (f & 1);
-  int j = (int)((f % (2 * L::NW)) >> 1);
-  nodes[f] = refit_chunk<K>(nodes, node, j, tets, vs, dt, true);
+  if (t >= count) return;
+  refit_node<K, true>(nodes, begin + t, tets, vs, dt);
 }
 
-// Levels [0, last] of the forest, deepest first, by a single block.
+// Levels [0, last] of the forest, deepest first, by a single block (plain
+// loads: the block reads records it wrote itself).
 template <int K>
 __global__ void __launch_bounds__(1024) refit_tail_kernel(float4* nodes, const int64_t* __restrict__ level_off,
                                                           int last, const uint4* __restrict__ tets,
                                                           VertexSource vs, DirTable dt) {
-  using L = NodeLayout<K>;
   for (int d = last; d >= 0; --d) {
-    int64_t b = level_off[d] * L::NW, e = level_off[d + 1] * L::NW;
-    for (int64_t f = b + threadIdx.x; f < e; f += blockDim.x) {
-      int64_t node = 2 * (f / (2 * L::NW)) + (f & 1);
-      int j = (int)((f % (2 * L::NW)) >> 1);
-      nodes[f] = refit_chunk<K>(nodes, node, j, tets, vs, dt, false);
-    }
+    for (int64_t n = level_off[d] + threadIdx.x; n < level_off[d + 1]; n += blockDim.x)
+      refit_node<K, false>(nodes, n, tets, vs, dt);
     __syncthreads();
   }
 }
@@ -229,22 +216,20 @@ static const int64_t* level_off_dev(kdop_scene* s) {
 
 template <int K>
 static cudaError_t refit_impl(kdop_scene* s, int mode) {
-  using L = NodeLayout<K>;
   VertexSource vs = vertex_source(s, mode);
-  const int64_t small = 16384;
+  const int64_t small = 4096;  // nodes of a level refitted by the single-block kernel
   int levels = (int)s->level_off.size() - 1;
   if (levels <= 0) return cudaSuccess;
   int tail = -1;  // levels [0, tail] go to the single-block kernel
   for (int d = 0; d < levels; ++d) {
-    if ((s->level_off[d + 1] - s->level_off[d]) * L::NW <= small)
+    if (s->level_off[d + 1] - s->level_off[d] <= small)
       tail = d;
     else
       break;
   }
   for (int d = levels - 1; d > tail; --d) {
     int64_t b = s->level_off[d], n = s->level_off[d + 1] - b;
-    int64_t items = n * L::NW;
-    unsigned grid = (unsigned)((items + 255) / 256);
+    unsigned grid = (unsigned)((n + 255) / 256);
     refit_level_kernel<K><<<grid, 256, 0, s->ctx->stream>>>(s->nodes, b, n, s->tets, vs, s->dirs);
     s->ctx->launches++;
   }

@@ -156,7 +156,7 @@ struct Coop {
 // S sub-batches are loaded together per step, and one compaction per step
 // packs the pushes of all of them.
 template <int K, int C, int S>
-__global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
+__global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(TravArgs a) {
   using L = NodeLayout<K>;
   using CP = Coop<K, C>;
   constexpr int NW = L::NW;
@@ -183,19 +183,35 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
   int release = 0;       // work units taken and not yet released
   bool init_done = false;
   unsigned claim = 0xFFFFFFFFu;
-  unsigned long long my_tests = 0, my_lo = 0;
+  // per-lane counts, added to the control block's 64-bit totals every 1024
+  // steps and at the end (at most 4 per lane and step: no overflow)
+  unsigned tests32 = 0, lo32 = 0;
+  auto fold_counts = [&]() {
+    unsigned t = tests32, l = lo32;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      t += __shfl_down_sync(0xffffffffu, t, o);
+      l += __shfl_down_sync(0xffffffffu, l, o);
+    }
+    if (lane == 0) {
+      if (t) atomicAdd(&ctl->tests, (unsigned long long)t);
+      if (l) atomicAdd(&ctl->leaf_overlaps, (unsigned long long)l);
+    }
+    tests32 = lo32 = 0;
+  };
   unsigned max_depth = 0;
   bool failed = false;
 
   unsigned step = 0;
   for (;;) {
     // Queue counters for the donation check, read early so that their
-    // latency overlaps the node loads of this step: every step while the
-    // deque is deep, every 8th step while it holds a little work (so that
-    // the traversal's tail, when most warps wait, is spread again).
+    // latency overlaps the node loads of this step.
     unsigned q_h = 0, q_t = 0;
     ++step;
-    if (lane == 0 && (top - bot >= a.donate_min || (top - bot >= 2 && (step & 7u) == 0u))) {
+    if ((step & 1023u) == 0u) fold_counts();
+    // warp-uniform: poll the queue counters on every 4th step with work
+    const bool polled = top - bot >= 2 && (step & 3u) == 0u;
+    if (lane == 0 && polled) {
       q_h = ld_volatile(&ctl->q_head);
       q_t = ld_volatile(&ctl->q_tail);
     }
@@ -235,14 +251,14 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
             if (ra != NO_NODE && rb != NO_NODE) {
               uint32_t wa, wb;
               bool ov = node_overlap<K>(a.nodes, ra, rb, wa, wb);
-              my_tests += 1;
+              tests32 += 1u;
               if (ov) {
-                my_tests += 1;
+                tests32 += 1u;
                 pushA[0] = wa;
                 pushB[0] = wb;
                 slotP[0] = pid;
                 if (wa & wb & LEAF_BIT) {
-                  my_lo += 1;
+                  lo32 += 1u;
                   if (!a.surface_filter || (wa & wb & SURF_BIT)) emit_mask = 1;
                 } else {
                   push_mask = 1;
@@ -374,7 +390,7 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
         const uint32_t wB0 = __shfl_sync(0xffffffffu, t2, src);
         const uint32_t wB1 = __shfl_sync(0xffffffffu, t3, src);
         if (valid) {
-          if (gq == 0) my_tests += (unsigned long long)((singleA ? 1 : 2) * (singleB ? 1 : 2));
+          if (gq == 0) tests32 += (singleA ? 1u : 2u) * (singleB ? 1u : 2u);
 #pragma unroll
           for (int r = 0; r < PM; ++r) {
             const int c = gq + Q * r;
@@ -385,7 +401,7 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
             pushB[k] = wb;
             slotP[k] = ep[b];
             if (wa & wb & LEAF_BIT) {
-              my_lo += 1;
+              lo32 += 1u;
               if (!a.surface_filter || (wa & wb & SURF_BIT)) emit_mask |= 1u << k;
             } else {
               push_mask |= 1u << k;
@@ -467,7 +483,7 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
     // ---- donation: give the oldest entries to waiting warps ----
     // A deep deque gives to any waiting warp; while many warps wait (the
     // tail of the traversal) any deque with two or more entries gives half.
-    if (depth >= 2) {
+    if (polled && depth >= 2) {
       int waiting = 0;
       if (lane == 0) waiting = (q_h > q_t) ? (int)min(q_h - q_t, 1024u) : 0;
       waiting = __shfl_sync(0xffffffffu, waiting, 0);
@@ -496,14 +512,8 @@ __global__ void __launch_bounds__(512, 2) traverse_kernel(TravArgs a) {
   }
 
   // ---- totals ----
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    my_tests += __shfl_down_sync(0xffffffffu, my_tests, o);
-    my_lo += __shfl_down_sync(0xffffffffu, my_lo, o);
-  }
+  fold_counts();
   if (lane == 0) {
-    atomicAdd(&ctl->tests, my_tests);
-    atomicAdd(&ctl->leaf_overlaps, my_lo);
     atomicMax(&ctl->max_stack, max_depth);
     if (failed) atomicOr(&ctl->error, DEV_ERR_TIMEOUT);
   }
@@ -539,6 +549,8 @@ static cudaError_t prepare_k(size_t smem) {
     e = cudaFuncSetAttribute(traverse_kernel<K, 1, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(traverse_kernel<K, 2, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(traverse_kernel<K, 2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return e;
 }
 
@@ -621,10 +633,13 @@ static cudaError_t traverse_group(kdop_scene* s, int64_t n_pairs, const TravBuff
                                   int plain) {
   // load_group: 1 = one chunk pair per lane, one sub-batch per step;
   // 2 = two sub-batches per step; 4 = two chunk pairs per lane (half the
-  // lanes per entry, twice the entries per sub-batch)
+  // lanes per entry, twice the entries per sub-batch); 8 = two chunk pairs
+  // per lane and two sub-batches per step (twice the registers, one block
+  // per SM)
   switch (p.load_group) {
     case 1: return traverse_impl<K, 1, 1>(s, n_pairs, b, p, plain);
     case 4: return traverse_impl<K, 2, 1>(s, n_pairs, b, p, plain);
+    case 8: return traverse_impl<K, 2, 2>(s, n_pairs, b, p, plain);
     default: return traverse_impl<K, 1, 2>(s, n_pairs, b, p, plain);
   }
 }

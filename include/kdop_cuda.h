@@ -155,7 +155,8 @@ typedef struct {
   int32_t timeout_ms;     /* bound of every device-side wait (0: 5000) */
   int32_t load_group;     /* expansion shape (0: default 4): 1 = one 32-byte chunk pair per lane
                              and one batch of entries per step, 2 = two batches per step,
-                             4 = two chunk pairs per lane (half the lanes per entry) */
+                             4 = two chunk pairs per lane (half the lanes per entry),
+                             8 = 4 with two batches per step */
   int32_t wave_pairs;     /* pairs per persistent launch, largest first (0: all pairs in one launch) */
   int32_t smem_carveout;  /* shared-memory share of the L1/shared array in percent (0: driver choice) */
 } kdop_traverse_opts;
