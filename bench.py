@@ -42,7 +42,7 @@ UNIT = "node-pair tests/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--pairs", type=int, default=512)
@@ -126,6 +126,13 @@ class ClockSampler:
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
+
+    def wait_ready(self, timeout: float = 5.0):
+        """Block until nvidia-smi has printed its first sample (its start-up
+        takes a few hundred ms), so that the samples cover the timed region."""
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.01)
 
     def stop(self) -> dict:
         if not self.proc:
@@ -277,6 +284,7 @@ def run_cuda(args):
     dist.barrier()
     clocks = ClockSampler(dist.local)
     clocks.start()
+    clocks.wait_ready()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     ctx.synchronize()
