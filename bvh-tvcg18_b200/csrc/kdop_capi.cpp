@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "kdop_internal.h"
+#include "kdop_sort.h"
 
 using kdop::TravCtl;
 
@@ -69,6 +70,8 @@ cudaError_t launch_pack4(kdop_scene* s, const float* in, float4* out, int64_t n)
 struct kdop_scene_ext {
   float* stage = nullptr;
   int64_t stage_n = 0;
+  void* sort_work = nullptr;  // kdop_sort_results scratch
+  size_t sort_work_bytes = 0;
   std::vector<uint32_t> pairs_host;  // last traversed mesh pairs
   std::vector<uint32_t> order_host;  // their order of processing
   int64_t graph_kernels = 0;
@@ -222,6 +225,9 @@ static void scene_free(kdop_scene* s) {
   s->ctl_host = nullptr;
   if (x->stage) cudaFree(x->stage);
   x->stage = nullptr;
+  if (x->sort_work) cudaFree(x->sort_work);
+  x->sort_work = nullptr;
+  x->sort_work_bytes = 0;
 }
 
 // A captured graph holds the buffer addresses of its capture: any
@@ -820,6 +826,33 @@ int kdop_read_candidates(kdop_scene* s, uint32_t* rows, int64_t cap, int64_t* n_
     rows[3 * i + 1] = (uint32_t)((int64_t)h[i] - s->t_off[ma]);
     rows[3 * i + 2] = (uint32_t)((int64_t)h[n + i] - s->t_off[mb]);
   }
+  return KDOP_OK;
+}
+
+int kdop_sort_results(kdop_scene* s) {
+  if (!s) return KDOP_ERR_INVALID;
+  if (!s->traversed) return fail(s->ctx, KDOP_ERR_STATE, "kdop_sort_results before kdop_traverse");
+  kdop_stats st;
+  int rc = kdop_get_stats(s, &st);  // synchronises; reports overflow and device errors
+  if (rc != KDOP_OK) return rc;
+  int64_t n = std::min<int64_t>(st.n_candidates, s->cand_cap);
+  int64_t nc = s->contacted ? std::min<int64_t>(st.n_contacts, s->contact_cap) : 0;
+  if (n <= 0) return KDOP_OK;
+  kdop_scene_ext* x = ext(s);
+  size_t need = kdop::sort_results_bytes(n, nc);
+  if (x->sort_work_bytes < need) {
+    if (x->sort_work) {
+      cudaFree(x->sort_work);
+      s->device_bytes -= (int64_t)x->sort_work_bytes;
+    }
+    x->sort_work = nullptr;
+    x->sort_work_bytes = 0;
+    KDOP_CUDA(s->ctx, cudaMalloc(&x->sort_work, need));
+    x->sort_work_bytes = need;
+    s->device_bytes += (int64_t)need;
+  }
+  KDOP_CUDA(s->ctx, kdop::sort_results(s, n, nc, x->sort_work, s->ctx->stream));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
   return KDOP_OK;
 }
 

@@ -111,6 +111,7 @@ def load_library():
         "kdop_set_capacity": ([vp, i64, i64, i64], i32),
         "kdop_read_candidates": ([vp, vp, i64, C.POINTER(i64)], i32),
         "kdop_contacts": ([vp], i32),
+        "kdop_sort_results": ([vp], i32),
         "kdop_read_contacts": ([vp, vp, i64, C.POINTER(i64)], i32),
         "kdop_contacts_adjoint": ([vp, vp, vp, vp, i32], i32),
         "kdop_set_motion": ([vp, vp, vp, C.c_float, i32], i32),
@@ -339,6 +340,11 @@ class DeviceScene:
     # ---- contacts ----
     def contacts(self):
         self.ctx._check(self.lib.kdop_contacts(self.h), "kdop_contacts")
+
+    def sort_results(self):
+        """Reproducible order of the last traversal's results (device sort):
+        candidates by (pair, tet A, tet B), contacts grouped to match."""
+        self.ctx._check(self.lib.kdop_sort_results(self.h), "kdop_sort_results")
 
     def read_contacts(self) -> np.ndarray:
         st = self.stats(check=False)

@@ -240,6 +240,15 @@ int kdop_contacts(kdop_scene* scene);
  * reference's reporting order).  Synchronises. */
 int kdop_read_contacts(kdop_scene* scene, kdop_contact* rows, int64_t cap_rows, int64_t* n_rows);
 
+/* Puts the last traversal's results in a reproducible order, on the device:
+ * candidate rows by (pair, tet of A, tet of B) and, after kdop_contacts, the
+ * contact rows grouped by candidate in that order (each candidate's rows in
+ * the reference's reporting order), their `cand` fields, and the records the
+ * adjoint reads, to match.  Replaces the OpenCL back-end's result sort
+ * (cl/kdop_cl_tandem_traversal.h:1773-1788; the sequential back-end reports
+ * in traversal order).  Synchronises; not for stream capture. */
+int kdop_sort_results(kdop_scene* scene);
+
 /* Adjoint of contact generation with the pair set and every discrete choice
  * of the last kdop_contacts held fixed: given dL/d(depth) and dL/d(normal)
  * per contact row (n_contacts and n_contacts*3 floats; dn may be NULL),
