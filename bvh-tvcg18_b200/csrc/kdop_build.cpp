@@ -76,6 +76,22 @@ int direction_table(int K, float* o) {
   return -1;
 }
 
+// The integer scale of kdop_mesh_reorder.h's quantisation: min over the
+// three axes of (int)((float)(2^21 - 1) / (max - min)).  Returns false when a
+// quotient is not finite or beyond int range (the reference converts it
+// anyway; the host then keeps whatever its own conversion gives).
+bool morton_scale(const float* mn, const float* mx, int& scale) {
+  const int KB = (int)(sizeof(unsigned long long) * 8) / 3;
+  bool ok = true;
+  for (int d = 0; d < 3; ++d) {
+    float q = (float)((1 << KB) - 1) / (mx[d] - mn[d]);
+    if (!(q < 2147483520.0f && q > -2147483520.0f)) ok = false;
+    int v = (int)q;
+    scale = d == 0 ? v : std::min(scale, v);
+  }
+  return ok;
+}
+
 // Morton order of kdop_mesh_reorder.h:173-353, with its arithmetic: float
 // centroid sums scaled by the double 0.25, 21-bit quantisation with an integer
 // scale, the initial maximum numeric_limits<float>::min(), and std::sort on the
@@ -101,9 +117,8 @@ void morton_order(const float* xyz, int64_t nt, const uint32_t* tets, std::vecto
     }
   }
   const int KB = (int)(sizeof(unsigned long long) * 8) / 3;
-  int scale = (int)((float)((1 << KB) - 1) / (mx[0] - mn[0]));
-  scale = std::min(scale, (int)((float)((1 << KB) - 1) / (mx[1] - mn[1])));
-  scale = std::min(scale, (int)((float)((1 << KB) - 1) / (mx[2] - mn[2])));
+  int scale = 0;
+  morton_scale(mn, mx, scale);
   std::vector<std::pair<uint32_t, unsigned long long> > mc((size_t)nt);
   for (int64_t t = 0; t < nt; ++t) {
     unsigned long long x = (unsigned long long)(float)(int)((c[3 * t + 0] - mn[0]) * (float)scale);
@@ -188,28 +203,6 @@ void build_levels(const float* xyz, int64_t nt, const uint32_t* tets, const uint
   }
 }
 
-template <typename F>
-void parallel_for(int n, F fn) {
-  int th = (int)std::thread::hardware_concurrency();
-  if (th < 1) th = 1;
-  if (th > 64) th = 64;
-  if (th > n) th = n;
-  if (th <= 1) {
-    for (int i = 0; i < n; ++i) fn(i);
-    return;
-  }
-  std::vector<std::thread> pool;
-  std::atomic<int> next(0);
-  for (int t = 0; t < th; ++t)
-    pool.emplace_back([&]() {
-      for (;;) {
-        int i = next.fetch_add(1);
-        if (i >= n) break;
-        fn(i);
-      }
-    });
-  for (auto& t : pool) t.join();
-}
 }  // namespace
 
 int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t>& n_verts,
@@ -274,6 +267,54 @@ int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t
     out.topo[2 * (size_t)n_roots] = out.topo[0];
     out.topo[2 * (size_t)n_roots + 1] = out.topo[1];
   }
+  return 0;
+}
+
+// Level layout of the forest from the tet counts alone.  The index-median
+// split halves a range into ceil(s/2), floor(s/2), so the sizes at depth d
+// are floor or ceil of n / 2^d: depths 0 .. L = floor(log2 n) are complete
+// (2^d nodes) and depth L + 1 holds the 2 (n - 2^L) children of the size-2
+// nodes of depth L.  pre[d * (nm + 1) + m] = nodes of trees < m at level d.
+int forest_layout(const std::vector<int64_t>& n_tets, ForestBuild& out, std::vector<int64_t>& pre,
+                  std::vector<int32_t>& lg) {
+  const int nm = (int)n_tets.size();
+  lg.assign((size_t)nm, -1);
+  int levels = 0;
+  for (int m = 0; m < nm; ++m) {
+    int64_t n = n_tets[m];
+    if (n <= 0) continue;
+    int L = 0;
+    while ((int64_t(1) << (L + 1)) <= n) ++L;
+    lg[m] = L;
+    levels = std::max(levels, L + 1 + ((int64_t(1) << L) < n ? 1 : 0));
+  }
+  auto count = [&](int m, int d) -> int64_t {
+    int L = lg[m];
+    if (L < 0) return 0;
+    if (d <= L) return int64_t(1) << d;
+    if (d == L + 1) return 2 * (n_tets[m] - (int64_t(1) << L));
+    return 0;
+  };
+  pre.assign((size_t)levels * (nm + 1), 0);
+  std::vector<int64_t> tot((size_t)levels, 0);
+  for (int d = 0; d < levels; ++d) {
+    int64_t acc = 0;
+    for (int m = 0; m < nm; ++m) {
+      pre[(size_t)d * (nm + 1) + m] = acc;
+      acc += count(m, d);
+    }
+    pre[(size_t)d * (nm + 1) + nm] = acc;
+    tot[d] = acc;
+  }
+  if (levels > 0 && (tot[0] & 1)) tot[0] += 1;  // even root level (twin records)
+  out.level_off.assign((size_t)levels + 1, 0);
+  for (int d = 0; d < levels; ++d) out.level_off[d + 1] = out.level_off[d] + tot[d];
+  if (out.level_off[levels] >= (int64_t)(LEAF_BIT_HOST >> 1)) return -1;
+  out.root.assign((size_t)nm, 0xFFFFFFFFu);
+  for (int m = 0; m < nm; ++m)
+    if (lg[m] >= 0) out.root[m] = (uint32_t)pre[m];
+  out.depth = levels > 0 ? levels - 1 : 0;
+  out.topo.clear();
   return 0;
 }
 

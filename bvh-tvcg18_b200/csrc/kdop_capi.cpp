@@ -291,7 +291,13 @@ static int grow_pairs(kdop_scene* s, int64_t n) {
 }
 
 int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* meshes, kdop_scene** out) {
+  return kdop_scene_create_ex(ctx, K, n_meshes, meshes, KDOP_BUILD_DEVICE, out);
+}
+
+int kdop_scene_create_ex(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* meshes, int build,
+                         kdop_scene** out) {
   if (!ctx || !out) return KDOP_ERR_INVALID;
+  if (build != KDOP_BUILD_DEVICE && build != KDOP_BUILD_HOST) return fail(ctx, KDOP_ERR_INVALID, "unknown build mode");
   *out = nullptr;
   if (!valid_K(K)) return fail(ctx, KDOP_ERR_INVALID, "K must be one of 6, 8, 12, 14, 18, 20, 26");
   if (n_meshes < 0 || (n_meshes > 0 && !meshes)) return fail(ctx, KDOP_ERR_INVALID, "bad mesh list");
@@ -350,10 +356,15 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
     nts[m] = meshes[m].n_tets;
   }
   kdop::ForestBuild fb;
-  if (kdop::build_forest(xyz, nvs, tets, nts, orders, s->t_off, fb) != 0) {
+  std::vector<int64_t> pre;
+  std::vector<int32_t> lg;
+  int brc = build == KDOP_BUILD_HOST ? kdop::build_forest(xyz, nvs, tets, nts, orders, s->t_off, fb)
+                                     : kdop::forest_layout(nts, fb, pre, lg);
+  if (brc != 0) {
     delete box;
     return fail(ctx, KDOP_ERR_INVALID, "scene too large for 30-bit node indices");
   }
+  s->build = build;
   s->level_off = fb.level_off;
   s->root = fb.root;
   s->nn = fb.level_off.empty() ? 0 : fb.level_off.back();
@@ -363,7 +374,7 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
   std::vector<float4> rest((size_t)std::max<int64_t>(nv, 1));
   std::vector<uint4> gt((size_t)std::max<int64_t>(nt, 1));
   std::vector<uint8_t> surf((size_t)std::max<int64_t>(nt, 1));
-  for (int m = 0; m < n_meshes; ++m) {
+  kdop::parallel_for(n_meshes, [&](int m) {
     const kdop_mesh_desc& d = meshes[m];
     int mid = m;
     float midf;
@@ -378,11 +389,12 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
       std::memcpy(&surf[s->t_off[m]], d.surface, (size_t)d.n_tets);
     else if (d.n_tets)
       kdop::surface_map(d.n_tets, d.tets, &surf[s->t_off[m]]);
-  }
+  });
 
   int rc = KDOP_OK;
   cudaStream_t st = ctx->stream;
   uint32_t* topo_dev = nullptr;
+  uint32_t* perm_dev = nullptr;
   do {
     cudaError_t e;
 #define SC_TRY(call)                                 \
@@ -423,8 +435,34 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
     SC_TRY(cudaMemcpyAsync(s->ang_vel, z.data(), (size_t)n_meshes * sizeof(float4), cudaMemcpyHostToDevice, st));
     SC_TRY(cudaMemsetAsync(s->phase_dev, 0, sizeof(float), st));
     SC_TRY(cudaMemsetAsync(s->ctl, 0, sizeof(TravCtl), st));
-    SC_TRY(cudaMalloc((void**)&topo_dev, std::max<size_t>(fb.topo.size(), 1) * 4));
-    SC_TRY(cudaMemcpyAsync(topo_dev, fb.topo.data(), fb.topo.size() * 4, cudaMemcpyHostToDevice, st));
+    SC_TRY(cudaMalloc((void**)&topo_dev, (size_t)std::max<int64_t>(2 * s->nn, 1) * 4));
+    if (build == KDOP_BUILD_HOST) {
+      SC_TRY(cudaMemcpyAsync(topo_dev, fb.topo.data(), fb.topo.size() * 4, cudaMemcpyHostToDevice, st));
+    } else {
+      // leaf order on the device; caller-given orders and meshes whose Morton
+      // codes tie take the host's order
+      SC_TRY(cudaMalloc((void**)&perm_dev, (size_t)std::max<int64_t>(nt, 1) * 4));
+      std::vector<char> need_host;
+      SC_TRY(kdop::device_morton_perm(s, perm_dev, need_host));
+      std::vector<int> hm;
+      for (int m = 0; m < n_meshes; ++m)
+        if (meshes[m].n_tets > 0 && (meshes[m].leaf_order || need_host[m])) hm.push_back(m);
+      std::vector<std::vector<uint32_t> > hperm(hm.size());
+      kdop::parallel_for((int)hm.size(), [&](int k) {
+        int m = hm[k];
+        if (meshes[m].leaf_order)
+          hperm[k].assign(meshes[m].leaf_order, meshes[m].leaf_order + meshes[m].n_tets);
+        else
+          kdop::morton_order(meshes[m].xyz, meshes[m].n_tets, meshes[m].tets, hperm[k]);
+        for (auto& t : hperm[k]) t += (uint32_t)s->t_off[m];
+      });
+      for (size_t k = 0; k < hm.size(); ++k)
+        SC_TRY(cudaMemcpyAsync(perm_dev + s->t_off[hm[k]], hperm[k].data(), hperm[k].size() * 4,
+                               cudaMemcpyHostToDevice, st));
+      if (rc != KDOP_OK) break;
+      SC_TRY(kdop::device_topology(s, fb, pre, lg, perm_dev, topo_dev));
+      s->host_orders = (int)hm.size();
+    }
     SC_TRY(kdop::launch_write_topology(s, topo_dev));
     // make_tree ends with a refit (kdop_make_tree.h:285)
     SC_TRY(kdop::launch_refit(s, KDOP_REFIT_VERTICES));
@@ -434,6 +472,7 @@ int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* 
 #undef SC_TRY
   } while (0);
   if (topo_dev) cudaFree(topo_dev);
+  if (perm_dev) cudaFree(perm_dev);
   if (rc == KDOP_OK) rc = grow_candidates(s, kDefaultCand);
   if (rc == KDOP_OK) rc = grow_contacts(s, kDefaultContacts);
   if (rc == KDOP_OK) rc = grow_queue(s, kDefaultQueue);
@@ -468,6 +507,8 @@ int kdop_scene_get_info(const kdop_scene* s, kdop_scene_info* info) {
   info->n_nodes = s->nn;
   info->depth = s->depth;
   info->node_bytes = s->NW * 16;
+  info->build = s->build;
+  info->host_orders = s->host_orders;
   info->device_bytes = s->device_bytes;
   return KDOP_OK;
 }

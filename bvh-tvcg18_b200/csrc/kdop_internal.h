@@ -4,6 +4,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <thread>
 #include <limits>
 #include <map>
 #include <string>
@@ -123,6 +124,7 @@ struct kdop_scene {
   kdop::TravCtl* ctl = nullptr;
   kdop::TravCtl* ctl_host = nullptr;  // pinned
 
+  int host_orders = 0;  // meshes whose leaf order came from the host (device build)
   int refit_mode = -1;
   bool traversed = false;
   bool contacted = false;
@@ -133,9 +135,34 @@ struct kdop_scene {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
   int64_t device_bytes = 0;
+  int build = 0;  // KDOP_BUILD_DEVICE or KDOP_BUILD_HOST
 };
 
 namespace kdop {
+
+// fn(0 .. n-1) on up to 64 host threads
+template <typename F>
+inline void parallel_for(int n, F fn) {
+  int th = (int)std::thread::hardware_concurrency();
+  if (th < 1) th = 1;
+  if (th > 64) th = 64;
+  if (th > n) th = n;
+  if (th <= 1) {
+    for (int i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::vector<std::thread> pool;
+  std::atomic<int> next(0);
+  for (int t = 0; t < th; ++t)
+    pool.emplace_back([&]() {
+      for (;;) {
+        int i = next.fetch_add(1);
+        if (i >= n) break;
+        fn(i);
+      }
+    });
+  for (auto& t : pool) t.join();
+}
 
 // host tree construction (kdop_build.cpp)
 int direction_table(int K, float* out);
@@ -150,6 +177,22 @@ int build_forest(const std::vector<const float*>& xyz, const std::vector<int64_t
                  const std::vector<const uint32_t*>& tets, const std::vector<int64_t>& n_tets,
                  const std::vector<const uint32_t*>& orders, const std::vector<int64_t>& t_off, ForestBuild& out);
 void morton_order(const float* xyz, int64_t n_tets, const uint32_t* tets, std::vector<uint32_t>& perm);
+// Level offsets, roots and per-level tree offsets (pre: levels x (meshes + 1))
+// of the forest from the tet counts; lg[m] = floor(log2 n_tets[m]) or -1.
+int forest_layout(const std::vector<int64_t>& n_tets, ForestBuild& out, std::vector<int64_t>& pre,
+                  std::vector<int32_t>& lg);
+// Morton scale of kdop_mesh_reorder.h from a mesh's centroid bounds; false
+// when the reference's integer conversion would overflow.
+bool morton_scale(const float* mn, const float* mx, int& scale);
+// Device build of the leaf order: Morton codes of the rest centroids sorted
+// per mesh on the GPU (ties by tet index); meshes whose codes tie, or whose
+// scale degenerates, are flagged for the host order (std::sort's).
+// perm (nt): global tet ids, mesh by mesh in leaf order.
+cudaError_t device_morton_perm(kdop_scene* s, uint32_t* perm, std::vector<char>& need_host);
+// Topology (m_start, m_end per node, global ids) of the forest from its
+// layout and the leaf order perm; topo: 2 nn words.
+cudaError_t device_topology(kdop_scene* s, const ForestBuild& fb, const std::vector<int64_t>& pre,
+                            const std::vector<int32_t>& lg, const uint32_t* perm, uint32_t* topo);
 void surface_map(int64_t n_tets, const uint32_t* tets, uint8_t* surf);
 
 // kernel launchers (return cudaGetLastError of the launches)

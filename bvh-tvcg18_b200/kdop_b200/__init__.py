@@ -9,9 +9,9 @@ from __future__ import annotations
 
 from .lib import (KdopError, Context, DeviceScene, TraverseOpts, Stats, CONTACT_DTYPE, load_library,
                   library_path, REFIT_VERTICES, REFIT_POSE, REFIT_DEFORM, TRAVERSE_BATCHED, TRAVERSE_PLAIN,
-                  HOST, DEVICE)
+                  HOST, DEVICE, BUILD_DEVICE, BUILD_HOST)
 from . import scenes
 
 __all__ = ["KdopError", "Context", "DeviceScene", "TraverseOpts", "Stats", "CONTACT_DTYPE", "load_library",
            "library_path", "REFIT_VERTICES", "REFIT_POSE", "REFIT_DEFORM", "TRAVERSE_BATCHED", "TRAVERSE_PLAIN",
-           "HOST", "DEVICE", "scenes"]
+           "HOST", "DEVICE", "BUILD_DEVICE", "BUILD_HOST", "scenes"]

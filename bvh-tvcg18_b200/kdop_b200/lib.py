@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 HOST, DEVICE = 0, 1
 REFIT_VERTICES, REFIT_POSE, REFIT_DEFORM = 0, 1, 2
 TRAVERSE_BATCHED, TRAVERSE_PLAIN = 0, 1
+BUILD_DEVICE, BUILD_HOST = 0, 1
 
 _STATUS = {0: "ok", -1: "invalid argument", -2: "capacity exceeded", -3: "CUDA error",
            -4: "device wait timed out", -5: "out of memory", -6: "call out of order"}
@@ -44,7 +45,7 @@ class MeshDesc(C.Structure):
 class SceneInfo(C.Structure):
     _fields_ = [("K", C.c_int32), ("n_meshes", C.c_int32), ("n_verts", C.c_int64), ("n_tets", C.c_int64),
                 ("n_nodes", C.c_int64), ("depth", C.c_int32), ("node_bytes", C.c_int32),
-                ("device_bytes", C.c_int64)]
+                ("device_bytes", C.c_int64), ("build", C.c_int32), ("host_orders", C.c_int32)]
 
 
 class TraverseOpts(C.Structure):
@@ -96,6 +97,7 @@ def load_library():
         "kdop_ctx_synchronize": ([vp], i32),
         "kdop_ctx_launch_count": ([vp], i64),
         "kdop_scene_create": ([vp, i32, i32, C.POINTER(MeshDesc), C.POINTER(vp)], i32),
+        "kdop_scene_create_ex": ([vp, i32, i32, C.POINTER(MeshDesc), i32, C.POINTER(vp)], i32),
         "kdop_scene_destroy": ([vp], i32),
         "kdop_scene_get_info": ([vp, C.POINTER(SceneInfo)], i32),
         "kdop_read_tree": ([vp, i32, i64, vp, vp, C.POINTER(i64)], i32),
@@ -207,7 +209,8 @@ class Context:
 class DeviceScene:
     """Meshes and their kDOP trees on the device (kdop_scene)."""
 
-    def __init__(self, ctx: Context, K: int, meshes: Sequence, surface: bool = True):
+    def __init__(self, ctx: Context, K: int, meshes: Sequence, surface: bool = True, build: int = 0):
+        """build: BUILD_DEVICE (trees built on the GPU) or BUILD_HOST."""
         self.ctx = ctx
         self.lib = ctx.lib
         self.K = K
@@ -227,7 +230,8 @@ class DeviceScene:
             self.v_off[i + 1] = self.v_off[i] + xyz.shape[0]
             self.t_off[i + 1] = self.t_off[i] + tets.shape[0]
         h = C.c_void_p()
-        ctx._check(self.lib.kdop_scene_create(ctx.h, K, len(meshes), descs, C.byref(h)), "kdop_scene_create")
+        ctx._check(self.lib.kdop_scene_create_ex(ctx.h, K, len(meshes), descs, build, C.byref(h)),
+                   "kdop_scene_create")
         self._keep = []
         self.h = h
         self.n_meshes = len(meshes)

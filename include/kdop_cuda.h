@@ -97,6 +97,17 @@ typedef struct {
  * 0, 1, ..., n_tets-1 reproduces make_tree's tree of a mesh as given (the
  * reference reorders meshes before building, kdop_mesh_reorder.h:364-387). */
 int kdop_scene_create(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* meshes, kdop_scene** out);
+
+/* Where the trees are built.  Both give the same trees (the reference's
+ * make_tree over the Morton-reordered mesh):
+ *   KDOP_BUILD_DEVICE (kdop_scene_create's choice): Morton codes and their
+ *     sort on the GPU, topology written by one GPU thread per node; a mesh
+ *     with equal Morton codes (whose order std::sort leaves to itself) or a
+ *     caller-given leaf_order takes its leaf order from the host;
+ *   KDOP_BUILD_HOST: everything on the host (std::sort per mesh). */
+enum { KDOP_BUILD_DEVICE = 0, KDOP_BUILD_HOST = 1 };
+int kdop_scene_create_ex(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_desc* meshes, int build,
+                         kdop_scene** out);
 int kdop_scene_destroy(kdop_scene* scene);
 
 typedef struct {
@@ -108,6 +119,8 @@ typedef struct {
   int32_t depth;        /* deepest level index over all trees */
   int32_t node_bytes;   /* bytes per node record: 4 K + 8 rounded up to 16 */
   int64_t device_bytes; /* device memory held by the scene */
+  int32_t build;        /* KDOP_BUILD_DEVICE or KDOP_BUILD_HOST */
+  int32_t host_orders;  /* device build: meshes whose leaf order came from the host */
 } kdop_scene_info;
 int kdop_scene_get_info(const kdop_scene* scene, kdop_scene_info* info);
 

@@ -11,9 +11,9 @@
 //       replaces kdop_tandem_traversal.h:198-226 (and the OpenCL overload of
 //       cl/kdop_cl_tandem_traversal.h:623): every pair's contacts go to its
 //       TestPair::m_callback, per pair in the order of its candidate tet pairs
-//       sorted by (tet of A, tet of B), each candidate's contacts in the
-//       reference's generation order (the OpenCL path sorted too,
-//       kdop_cl_tandem_traversal.h:1773-1788).
+//       sorted by (tet of A, tet of B) on the device (kdop_sort_results),
+//       each candidate's contacts in the reference's generation order (the
+//       OpenCL path sorted too, kdop_cl_tandem_traversal.h:1773-1788).
 //   kdop::refit_tree(Tree<T,K>&, T4Mesh const&, X, Y, Z, kdop::cuda const&)
 //       replaces kdop_refit_tree.h:120-162 for one-chunk trees (make_tree with
 //       mem_bytes = SIZE_MAX, the reference's gProximity set-up): the node
@@ -187,6 +187,7 @@ inline void tandem_traversal(std::vector<TestPair<V, K, T> >& work_pool, cuda co
                       (st.device_error & 2) ? 2 * st.queue_capacity : 0);
     if (rc != KDOP_OK) break;
   }
+  if (rc == KDOP_OK) rc = kdop_sort_results(sc);  // candidates by (pair, tet A, tet B), contacts to match
   std::vector<uint32_t> cand((size_t)st.n_candidates * 3 + 3);
   std::vector<kdop_contact> rows((size_t)st.n_contacts + 1);
   int64_t nc = 0, nr = 0;
@@ -194,23 +195,10 @@ inline void tandem_traversal(std::vector<TestPair<V, K, T> >& work_pool, cuda co
   if (rc == KDOP_OK) rc = kdop_read_contacts(sc, rows.data(), st.n_contacts, &nr);
   kdop_scene_destroy(sc);
   cuda_detail::check(tag.ctx, rc, "tandem_traversal");
-  // contacts per candidate, candidates per pair sorted by (tet A, tet B)
-  std::vector<std::vector<int64_t> > of_cand((size_t)nc);
-  for (int64_t r = 0; r < nr; ++r) of_cand[rows[r].cand].push_back(r);
-  std::vector<int64_t> order((size_t)nc);
-  for (int64_t i = 0; i < nc; ++i) order[i] = i;
-  std::sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
-    for (int k = 0; k < 3; ++k)
-      if (cand[3 * x + k] != cand[3 * y + k]) return cand[3 * x + k] < cand[3 * y + k];
-    return false;
-  });
-  for (size_t oi = 0; oi < order.size(); ++oi) {
-    int64_t ci = order[oi];
-    P& p = work_pool[cand[3 * ci]];
-    for (size_t k = 0; k < of_cand[ci].size(); ++k) {
-      kdop_contact const& c = rows[of_cand[ci][k]];
-      (*p.m_callback)(V::make(c.p[0], c.p[1], c.p[2]), V::make(c.n[0], c.n[1], c.n[2]), (T)c.depth);
-    }
+  for (int64_t r = 0; r < nr; ++r) {
+    kdop_contact const& c = rows[r];
+    P& p = work_pool[cand[3 * c.cand]];
+    (*p.m_callback)(V::make(c.p[0], c.p[1], c.p[2]), V::make(c.n[0], c.n[1], c.n[2]), (T)c.depth);
   }
 }
 
