@@ -14,18 +14,19 @@
 // kdop_cl_tandem_traversal.cl:19-233, and the gProximity queues,
 // cl/kernels/gproximity/*.cl):
 //   * one persistent launch sized to the resident-block count; each warp owns
-//     a node-pair deque in shared memory and pops up to 32 pairs per step, one
-//     per lane;
-//   * "test on expand": a popped entry is a pair already known to overlap; the
-//     lane loads the children records (the two children of a node are adjacent,
-//     so a 2-child side is one contiguous 2-record read, float4 by float4,
-//     stopping as soon as every child pair is separated), tests all child pairs
-//     and keeps the overlapping ones;
-//   * ballot/shuffle compaction: one warp-wide prefix sum packs the kept pairs
-//     into the deque and the leaf pairs into the output with one atomic per warp;
-//   * load balance: root pairs are claimed from the pair list, and a warp whose
-//     deque holds many pairs while other warps wait gives its oldest (largest)
-//     entries to a global queue; a deque overflow spills there too;
+//     a node-pair deque in shared memory;
+//   * "test on expand": a popped entry is a pair already known to overlap;
+//     a few lanes take one entry together and read the children of both sides
+//     as whole twin records (siblings' chunks interleaved, so one 256-bit load
+//     per lane and chunk pair), test the four child pairs slab by slab, and
+//     keep the overlapping ones (see traverse_kernel);
+//   * ballot compaction: prefix sums over per-lane push counts pack the kept
+//     pairs into the deque, and emitted leaf pairs reserve rows with one
+//     atomic per warp;
+//   * load balance: root pairs are claimed from the pair list (largest first),
+//     and a warp whose deque is deep while other warps wait gives its oldest
+//     (largest) entries to a global queue -- any deque with work gives half
+//     while many warps wait; a deque overflow spills there too;
 //   * termination: a global count of outstanding work units reaches zero;
 //     every wait is bounded by a time limit after which the kernel records
 //     DEV_ERR_TIMEOUT and returns (no unbounded spin).
