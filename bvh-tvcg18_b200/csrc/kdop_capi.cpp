@@ -680,6 +680,8 @@ int kdop_resolve_traverse_opts(const kdop_scene* s, const kdop_traverse_opts* o,
   p.smem_carveout = o->smem_carveout > 0 ? o->smem_carveout : (o->smem_carveout < 0 ? -1 : d.smem_carveout);
   if (p.wave_pairs < 0) p.wave_pairs = 0;
   if (p.smem_carveout < 0) p.smem_carveout = 0;
+  p.stuck_work = o->test_stuck_work;
+  if (p.stuck_work < 0 || p.stuck_work > 1024) return KDOP_ERR_INVALID;
   if (p.smem_carveout > 100) return KDOP_ERR_INVALID;
   if (p.block_warps > 16 || (p.stack_cap & (p.stack_cap - 1)) || p.stack_cap < 64 || p.init_chunk > 32)
     return KDOP_ERR_INVALID;

@@ -64,6 +64,7 @@ struct TravParams {
   int load_group;
   int wave_pairs;
   int smem_carveout;
+  int stuck_work;  // test hook: outstanding work units nobody completes
 };
 
 }  // namespace kdop

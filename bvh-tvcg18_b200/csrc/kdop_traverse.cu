@@ -520,7 +520,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
   }
 }
 
-__global__ void trav_init_kernel(TravCtl* c, unsigned n_init, unsigned pair_base, int reset_totals) {
+__global__ void trav_init_kernel(TravCtl* c, unsigned n_init, unsigned pair_base, int reset_totals, int stuck) {
   if (threadIdx.x != 0) return;
   if (reset_totals) {
     c->tests = 0;
@@ -533,7 +533,7 @@ __global__ void trav_init_kernel(TravCtl* c, unsigned n_init, unsigned pair_base
   c->init_head = 0;
   c->q_head = 0;
   c->q_tail = 0;
-  c->work = (int)n_init;
+  c->work = (int)n_init + stuck;
   c->n_init = n_init;
   c->pair_base = pair_base;
 }
@@ -610,19 +610,20 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
     if (wave < 1) wave = 1;
     for (int64_t off = 0; off < n_pairs || off == 0; off += wave) {
       int64_t n = std::min<int64_t>(wave, n_pairs - off);
-      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)std::max<int64_t>(n, 0), (unsigned)off, off == 0);
+      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)std::max<int64_t>(n, 0), (unsigned)off, off == 0,
+                                         p.stuck_work);
       traverse_kernel<K, C, S><<<grid, threads, smem, st>>>(a);
       s->ctx->launches += 2;
       if (n_pairs == 0) break;
     }
   } else {
     for (int64_t i = 0; i < n_pairs; ++i) {
-      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 1u, (unsigned)i, i == 0 ? 1 : 0);
+      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 1u, (unsigned)i, i == 0 ? 1 : 0, p.stuck_work);
       traverse_kernel<K, C, S><<<grid, threads, smem, st>>>(a);
       s->ctx->launches += 2;
     }
     if (n_pairs == 0) {
-      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 0u, 0u, 1);
+      trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, 0u, 0u, 1, 0);
       s->ctx->launches += 1;
     }
   }

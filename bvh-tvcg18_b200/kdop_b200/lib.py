@@ -52,7 +52,7 @@ class TraverseOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("surface_filter", C.c_int32), ("block_warps", C.c_int32),
                 ("stack_cap", C.c_int32), ("init_chunk", C.c_int32), ("donate_min", C.c_int32),
                 ("timeout_ms", C.c_int32), ("load_group", C.c_int32), ("wave_pairs", C.c_int32),
-                ("smem_carveout", C.c_int32)]
+                ("smem_carveout", C.c_int32), ("test_stuck_work", C.c_int32)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}

@@ -172,6 +172,9 @@ typedef struct {
                              8 = 4 with two batches per step */
   int32_t wave_pairs;     /* pairs per persistent launch, largest first (0: all pairs in one launch) */
   int32_t smem_carveout;  /* shared-memory share of the L1/shared array in percent (0: driver choice) */
+  int32_t test_stuck_work; /* test hook, normally 0: this many extra work units that never complete,
+                              so every waiting warp gives up after timeout_ms and the call reports
+                              KDOP_ERR_TIMEOUT (exercises the bounded waits without a GPU fault) */
 } kdop_traverse_opts;
 
 /* Fills opts with the defaults (or the autotuned choice cached for this scene). */
