@@ -45,7 +45,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
-    ap.add_argument("--pairs", type=int, default=512)
+    ap.add_argument("--pairs", type=int, default=0, help="mesh pairs per GPU (config3: 512, config5: 256)")
+    ap.add_argument("--workload", default="config3", choices=["config3", "config2", "config5", "config1"],
+                    help="config3 is the headline; the others are the same step on the other configs")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -180,7 +182,13 @@ def ncu_traffic(name: str):
 
 def workload(args, rank: int):
     from kdop_b200 import scenes
-    return scenes.config3(n_pairs=args.pairs, seed=2 + rank)
+    if args.workload == "config2":
+        return scenes.config2()
+    if args.workload == "config5":
+        return scenes.config5(n_pairs=args.pairs or 256)
+    if args.workload == "config1":
+        return scenes.config1()
+    return scenes.config3(n_pairs=args.pairs or 512, seed=2 + rank)
 
 
 def cpu_sample(sc, tests_per_pair, budget_tests):
@@ -320,7 +328,7 @@ def run_cuda(args):
     alg_bytes = tests_per_step * 2 * node_bytes
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (trav_ms * 1e-3) / 1e9
-    traffic = ncu_traffic("traverse_config3.md")
+    traffic = ncu_traffic("traverse_config3.md") if args.workload == "config3" else None
 
     # plain: one traversal launch per mesh pair, same trees and descent rule;
     # the faster of the default and the batched-tuned launch shape
@@ -419,7 +427,9 @@ def run_cuda(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": sc.name, "pairs_per_gpu": int(len(sc.pairs)), "tets_per_gpu": int(sc.n_tets),
                        "K": sc.K, "node_bytes": node_bytes, "parallelism": f"pairs sharded, {dist.world} rank(s)",
-                       "l2": f"inputs larger than L2 (node records {info['n_nodes'] * node_bytes / 1e9:.2f} GB)",
+                       "l2": (f"inputs larger than L2 (node records {info['n_nodes'] * node_bytes / 1e9:.2f} GB)"
+                              if info['n_nodes'] * node_bytes > 126e6 else
+                              f"inputs fit in L2 (node records {info['n_nodes'] * node_bytes / 1e6:.1f} MB), no flush"),
                        "step": "CUDA graph: pose transform + refit, batched traversal, contacts",
                        "tests_per_step_per_gpu": int(tests_per_step), "candidates": int(st2.n_candidates),
                        "contacts": int(st2.n_contacts), "traverse_opts": opts.as_dict(), "autotuned": tuned},

@@ -13,14 +13,16 @@
 //      all candidates, points projected on the mid plane, near-duplicates
 //      (max-norm < 10 FLT_EPSILON) dropped, reported in order (:622-681).
 //
-// Two passes.  A thread per candidate tet pair first runs steps 1 and 2 up
-// to the first separating axis or the first admissible face pair (almost all
-// leaf pairs of a deep overlap stop there: no contact) and lists the pairs
-// that go on.  Then one warp handles each listed pair: lanes evaluate the 44
-// SAT axes, the 16 face pairs and the 56 contact candidates in parallel;
-// ballots keep the reference's candidate order, so the reported rows and
-// every value equal the reference's FP32 results.  Both passes evaluate the
-// same functions on the same inputs, so their decisions agree.
+// Two passes, a thread per candidate tet pair in each.  The first runs steps
+// 1 and 2 up to the first separating axis or the first admissible face pair
+// (almost all leaf pairs of a deep overlap stop there: no contact) and lists
+// the pairs that go on; the second runs step 2's argmin and step 3 for the
+// listed pairs in the reference's order (face pairs, then the 56 candidates
+// in generation order), so the reported rows and every value equal the
+// reference's FP32 results.  Both passes evaluate the same functions on the
+// same inputs, so their decisions agree.  (A warp-per-pair form, lanes over
+// SAT axes, face pairs and candidates with ballots keeping the order, took
+// 1.5x longer on contact-rich pairs: most phases kept few lanes busy.)
 #include "kdop_device.cuh"
 
 namespace kdop {
@@ -136,11 +138,6 @@ __device__ __forceinline__ bool sat_test(int t, const f3* A, const f3* B) {
   return (hi_s < lo_u) || (lo_s > hi_u);
 }
 
-__device__ __forceinline__ f3 shfl3(f3 v, int src) {
-  return mk3(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src),
-             __shfl_sync(0xffffffffu, v.z, src));
-}
-
 struct ContactArgs {
   const uint32_t* candA;
   const uint32_t* candB;
@@ -155,8 +152,6 @@ struct ContactArgs {
   unsigned out_cap;
   TravCtl* ctl;
 };
-
-constexpr int WARPS_PER_BLOCK_C = 8;
 
 // Face pair (fa, fb) admissible as the most opposing pair (…_tetrahedron_
 // tetrahedron.h:465-533): both boundary faces, opposing unit normals, and
@@ -222,171 +217,124 @@ __global__ void __launch_bounds__(256) contacts_filter_kernel(ContactArgs a) {
   }
 }
 
-__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK_C) contacts_kernel(ContactArgs a) {
-  __shared__ float s_pts[WARPS_PER_BLOCK_C][56][3];
+// Pass 2, thread per listed pair: the argmin over the 16 face pairs by a
+// strict < in loop order (first occurrence), the 56 candidates in generation
+// order with running min / max of p.n (first occurrence), projection on the
+// mid plane, and the duplicate test of each candidate against every earlier
+// one.  Rows of a warp are placed with one atomic.
+__global__ void __launch_bounds__(128) contacts_thread_kernel(ContactArgs a) {
   const int lane = threadIdx.x & 31;
-  const int wib = threadIdx.x >> 5;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  unsigned n_surv = *(volatile unsigned*)&a.ctl->n_surv;
-  unsigned warp = blockIdx.x * WARPS_PER_BLOCK_C + wib;
-  unsigned n_warps = gridDim.x * WARPS_PER_BLOCK_C;
-  for (unsigned k = warp; k < n_surv; k += n_warps) {
-    const unsigned ci = a.surv[k];
-    uint32_t ta = a.candA[ci], tb = a.candB[ci];
+  const unsigned n_surv = *(volatile unsigned*)&a.ctl->n_surv;
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_surv; base += stride) {
+    const unsigned k = base + lane;
+    const bool act = k < n_surv;
+    unsigned ci = 0;
     int4 record = make_int4(-1, -1, 0, 0);
-    uint32_t sa = a.surf[ta], sb = a.surf[tb];
-    // vertices: lane l < 8 fetches vertex l (A0..A3, B0..B3)
-    uint4 qa = __ldg(a.tets + ta), qb = __ldg(a.tets + tb);
-    f3 mine = mk3(0.f, 0.f, 0.f);
-    if (lane < 8) {
-      uint32_t vid = (lane == 0) ? qa.x : (lane == 1) ? qa.y : (lane == 2) ? qa.z : (lane == 3) ? qa.w
-                   : (lane == 4) ? qb.x : (lane == 5) ? qb.y : (lane == 6) ? qb.z : qb.w;
-      mine = world_vertex(a.vs, vid);
-    }
-    f3 A[4], B[4];
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      A[v] = shfl3(mine, v);
-      B[v] = shfl3(mine, 4 + v);
-    }
-    bool ok = (sa != 0u) && (sb != 0u);
-    if (ok) {
-      // 1. exact overlap
-      bool sepr = sat_test(lane, A, B);
-      if (lane < 12) sepr = sepr || sat_test(32 + lane, A, B);
-      ok = !__any_sync(0xffffffffu, sepr);
-    }
-    if (ok) {
-      // unscaled face planes: lane l < 8 builds plane l (A faces 0-3, B faces 0-3)
-      UPlane mp{mk3(0.f, 0.f, 0.f), mk3(0.f, 0.f, 0.f)};
-      if (lane < 8) {
-        const f3* X = (lane < 4) ? A : B;
-        int f = lane & 3;
-        mp = unscaled_plane(X[c_face[f][0]], X[c_face[f][1]], X[c_face[f][2]]);
-      }
+    int nq = 0, nu = 0;
+    float depth = 0.f;
+    f3 n = mk3(0.f, 0.f, 0.f);
+    float px[56], py[56], pz[56];
+    uint64_t kept = 0;
+    if (act) {
+      ci = a.surv[k];
+      const uint32_t ta = a.candA[ci], tb = a.candB[ci];
+      const uint32_t sa = a.surf[ta], sb = a.surf[tb];
+      const uint4 qa = __ldg(a.tets + ta), qb = __ldg(a.tets + tb);
+      f3 A[4] = {world_vertex(a.vs, qa.x), world_vertex(a.vs, qa.y), world_vertex(a.vs, qa.z),
+                 world_vertex(a.vs, qa.w)};
+      f3 B[4] = {world_vertex(a.vs, qb.x), world_vertex(a.vs, qb.y), world_vertex(a.vs, qb.z),
+                 world_vertex(a.vs, qb.w)};
       UPlane PA[4], PB[4];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) {
-        PA[v].n = shfl3(mp.n, v);
-        PA[v].p = shfl3(mp.p, v);
-        PB[v].n = shfl3(mp.n, 4 + v);
-        PB[v].p = shfl3(mp.p, 4 + v);
+      for (int f = 0; f < 4; ++f) {
+        PA[f] = unscaled_plane(A[c_face[f][0]], A[c_face[f][1]], A[c_face[f][2]]);
+        PB[f] = unscaled_plane(B[c_face[f][0]], B[c_face[f][1]], B[c_face[f][2]]);
       }
-      // 2. most opposing boundary faces: lane l < 16 -> (a, b) = (l / 4, l % 4)
-      float test = 3.0e38f;
-      bool good = false;
-      f3 nA = mk3(0.f, 0.f, 0.f);
-      if (lane < 16) good = face_pair_ok(lane >> 2, lane & 3, sa, sb, PA, PB, A, B, test, nA);
-      // first (a, b) in loop order with the smallest value
-      float bv = good ? test : 3.0e38f;
-      int bl = good ? lane : 64;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        float ov = __shfl_xor_sync(0xffffffffu, bv, o);
-        int ol = __shfl_xor_sync(0xffffffffu, bl, o);
-        if (ov < bv || (ov == bv && ol < bl)) {
-          bv = ov;
-          bl = ol;
+      float bv = 3.0e38f;
+      int bl = -1;
+      for (int l = 0; l < 16; ++l) {
+        float t;
+        f3 nA;
+        if (face_pair_ok(l >> 2, l & 3, sa, sb, PA, PB, A, B, t, nA) && t < bv) {
+          bv = t;
+          bl = l;
+          n = nA;
         }
       }
-      if (bl < 64) {
-        f3 n = shfl3(nA, bl);
+      if (bl >= 0) {
         record.x = bl >> 2;
         record.y = 0;
-        // 3. contact candidates, codes lane and lane + 32
-        f3 q0, q1;
-        bool h0 = candidate(lane, A, B, PA, PB, q0);
-        bool h1 = (lane < 24) ? candidate(32 + lane, A, B, PA, PB, q1) : false;
-        unsigned m0 = __ballot_sync(0xffffffffu, h0);
-        unsigned m1 = __ballot_sync(0xffffffffu, h1);
-        int n0 = __popc(m0);
-        int nq = n0 + __popc(m1);
+        float mnv = 0.f, mxv = 0.f;
+        int mnc = -1, mxc = -1;
+        for (int c = 0; c < 56; ++c) {
+          f3 q;
+          if (!candidate(c, A, B, PA, PB, q)) continue;
+          const float d = dot3(q, n);
+          if (nq == 0 || d < mnv) { mnv = d; mnc = c; }
+          if (nq == 0 || mxv < d) { mxv = d; mxc = c; }
+          px[nq] = q.x;
+          py[nq] = q.y;
+          pz[nq] = q.z;
+          ++nq;
+        }
         if (nq > 0) {
-          int pos0 = __popc(m0 & lt_mask), pos1 = n0 + __popc(m1 & lt_mask);
-          float d0 = h0 ? dot3(q0, n) : 0.f, d1 = h1 ? dot3(q1, n) : 0.f;
-          // min and max with the position of their first occurrence
-          float mnv = 3.0e38f, mxv = -3.0e38f;
-          int mnp = 1 << 20, mxp = 1 << 20, mnc = -1, mxc = -1;
-          if (h0) {
-            mnv = d0; mnp = pos0; mnc = lane;
-            mxv = d0; mxp = pos0; mxc = lane;
-          }
-          if (h1 && (d1 < mnv || !h0)) { mnv = d1; mnp = pos1; mnc = 32 + lane; }
-          if (h1 && (mxv < d1 || !h0)) { mxv = d1; mxp = pos1; mxc = 32 + lane; }
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            float ov = __shfl_xor_sync(0xffffffffu, mnv, o);
-            int op = __shfl_xor_sync(0xffffffffu, mnp, o);
-            int oc = __shfl_xor_sync(0xffffffffu, mnc, o);
-            if (ov < mnv || (ov == mnv && op < mnp)) { mnv = ov; mnp = op; mnc = oc; }
-            ov = __shfl_xor_sync(0xffffffffu, mxv, o);
-            op = __shfl_xor_sync(0xffffffffu, mxp, o);
-            oc = __shfl_xor_sync(0xffffffffu, mxc, o);
-            if (mxv < ov || (ov == mxv && op < mxp)) { mxv = ov; mxp = op; mxc = oc; }
-          }
-          float depth = fsub(mnv, mxv);
-          float ssum = fadd(mxv, mnv);
-          f3 mid = mk3(fmul(fmul(n.x, ssum), 0.5f), fmul(fmul(n.y, ssum), 0.5f), fmul(fmul(n.z, ssum), 0.5f));
-          if (h0) {
-            float k = dot3(n, sub3(q0, mid));
-            q0 = sub3(q0, mk3(fmul(k, n.x), fmul(k, n.y), fmul(k, n.z)));
-            s_pts[wib][pos0][0] = q0.x; s_pts[wib][pos0][1] = q0.y; s_pts[wib][pos0][2] = q0.z;
-          }
-          if (h1) {
-            float k = dot3(n, sub3(q1, mid));
-            q1 = sub3(q1, mk3(fmul(k, n.x), fmul(k, n.y), fmul(k, n.z)));
-            s_pts[wib][pos1][0] = q1.x; s_pts[wib][pos1][1] = q1.y; s_pts[wib][pos1][2] = q1.z;
-          }
-          __syncwarp();
+          depth = fsub(mnv, mxv);
+          const float ssum = fadd(mxv, mnv);
+          const f3 mid = mk3(fmul(fmul(n.x, ssum), 0.5f), fmul(fmul(n.y, ssum), 0.5f), fmul(fmul(n.z, ssum), 0.5f));
           const float eps = 1.1920928955078125e-06f;  // 10 * FLT_EPSILON
-          bool u0 = h0, u1 = h1;
-          for (int j = 0; j < nq; ++j) {
-            float px = s_pts[wib][j][0], py = s_pts[wib][j][1], pz = s_pts[wib][j][2];
-            if (u0 && j < pos0) {
-              float m = smax(smax(fabsf(fsub(px, q0.x)), fabsf(fsub(py, q0.y))), fabsf(fsub(pz, q0.z)));
-              if (m < eps) u0 = false;
+          for (int i = 0; i < nq; ++i) {
+            f3 q = mk3(px[i], py[i], pz[i]);
+            const float kk = dot3(n, sub3(q, mid));
+            q = sub3(q, mk3(fmul(kk, n.x), fmul(kk, n.y), fmul(kk, n.z)));
+            px[i] = q.x;
+            py[i] = q.y;
+            pz[i] = q.z;
+            bool u = true;
+            for (int j = 0; j < i && u; ++j) {
+              float m = smax(smax(fabsf(fsub(px[j], q.x)), fabsf(fsub(py[j], q.y))), fabsf(fsub(pz[j], q.z)));
+              if (m < eps) u = false;
             }
-            if (u1 && j < pos1) {
-              float m = smax(smax(fabsf(fsub(px, q1.x)), fabsf(fsub(py, q1.y))), fabsf(fsub(pz, q1.z)));
-              if (m < eps) u1 = false;
-            }
-          }
-          unsigned um0 = __ballot_sync(0xffffffffu, u0);
-          unsigned um1 = __ballot_sync(0xffffffffu, u1);
-          int nu0 = __popc(um0), nu = nu0 + __popc(um1);
-          unsigned base = 0;
-          if (lane == 0) base = atomicAdd(&a.ctl->n_contacts, (unsigned)nu);
-          base = __shfl_sync(0xffffffffu, base, 0);
-          if (u0) {
-            unsigned r = base + __popc(um0 & lt_mask);
-            if (r < a.out_cap) {
-              kdop_contact c;
-              c.p[0] = q0.x; c.p[1] = q0.y; c.p[2] = q0.z;
-              c.n[0] = n.x; c.n[1] = n.y; c.n[2] = n.z;
-              c.depth = depth;
-              c.cand = ci;
-              a.out[r] = c;
-            }
-          }
-          if (u1) {
-            unsigned r = base + nu0 + __popc(um1 & lt_mask);
-            if (r < a.out_cap) {
-              kdop_contact c;
-              c.p[0] = q1.x; c.p[1] = q1.y; c.p[2] = q1.z;
-              c.n[0] = n.x; c.n[1] = n.y; c.n[2] = n.z;
-              c.depth = depth;
-              c.cand = ci;
-              a.out[r] = c;
+            if (u) {
+              kept |= 1ull << i;
+              ++nu;
             }
           }
           record.y = (mnc & 0xFF) | ((mxc & 0xFF) << 8);
           record.z = nu;
-          record.w = (int)base;
-          __syncwarp();
         }
       }
     }
-    if (lane == 0) a.rec[ci] = record;
+    // rows of the warp: one atomic
+    int incl = nu;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned wbase = 0;
+    if (lane == 0 && total > 0) wbase = atomicAdd(&a.ctl->n_contacts, (unsigned)total);
+    wbase = __shfl_sync(0xffffffffu, wbase, 0);
+    if (act) {
+      if (nu > 0) {
+        unsigned r = wbase + (unsigned)(incl - nu);
+        record.w = (int)r;
+        for (int i = 0; i < nq; ++i) {
+          if (!((kept >> i) & 1ull)) continue;
+          if (r < a.out_cap) {
+            kdop_contact c;
+            c.p[0] = px[i]; c.p[1] = py[i]; c.p[2] = pz[i];
+            c.n[0] = n.x; c.n[1] = n.y; c.n[2] = n.z;
+            c.depth = depth;
+            c.cand = ci;
+            a.out[r] = c;
+          }
+          ++r;
+        }
+      }
+      a.rec[ci] = record;
+    }
   }
 }
 
@@ -566,7 +514,7 @@ cudaError_t launch_contacts(kdop_scene* s) {
   contacts_reset_kernel<<<1, 32, 0, s->ctx->stream>>>(s->ctl);
   unsigned grid = (unsigned)s->ctx->sm_count * 8u;
   contacts_filter_kernel<<<grid, 256, 0, s->ctx->stream>>>(a);
-  contacts_kernel<<<grid, 32 * WARPS_PER_BLOCK_C, 0, s->ctx->stream>>>(a);
+  contacts_thread_kernel<<<grid * 2, 128, 0, s->ctx->stream>>>(a);
   s->ctx->launches += 3;
   return cudaGetLastError();
 }
