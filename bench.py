@@ -210,14 +210,15 @@ def oracle_tests_per_pair(sc, threads=0):
     return tpp
 
 
-def reference_time(sc, n_pairs, threads):
+def reference_time(sc, n_pairs, threads, repeats=1):
     from oracle.pyoracle import RefTimer
     R = RefTimer()
     used = sorted(set(sc.pairs[:n_pairs].ravel().tolist()))
     remap = {m: i for i, m in enumerate(used)}
     meshes = [sc.meshes[m] for m in used]
     pairs = np.array([[remap[a], remap[b]] for a, b in sc.pairs[:n_pairs]], np.uint32)
-    sec, contacts = R.time_pairs(sc.K, meshes, sc.quat[used], sc.pos[used], pairs, threads=threads)
+    sec, contacts = R.time_pairs(sc.K, meshes, sc.quat[used], sc.pos[used], pairs, threads=threads,
+                                 repeats=repeats)
     return sec, contacts
 
 
@@ -234,13 +235,13 @@ def run_reference(args):
     threads = os.cpu_count() or 1
     sc = workload(args, 0)
     tpp = oracle_tests_per_pair(sc)
-    # per step: a bounded sample of the workload, sized for ~4 s on all threads
-    n, tests = cpu_sample(sc, tpp, budget_tests=4.0 * 30e6 * threads)
-    times = []
-    for i in range(args.warmup + args.steps):
-        sec, _ = reference_time(sc, n, threads)
-        if i >= args.warmup:
-            times.append(sec)
+    # per step: a bounded sample of the workload, sized so that the whole run
+    # takes about 90 s on all threads (at most 4 s a step)
+    per_step_s = min(4.0, 90.0 / max(args.steps + args.warmup, 1))
+    n, tests = cpu_sample(sc, tpp, budget_tests=per_step_s * 30e6 * threads)
+    reps = args.warmup + max(args.steps, 1)
+    secs, _ = reference_time(sc, n, threads, repeats=reps)
+    times = (secs if isinstance(secs, list) else [secs])[args.warmup:]
     t = sum(times) / len(times)
     value = tests / t
     sample = f"first {n} of {len(sc.pairs)} pairs per step ({tests} node-pair tests)"

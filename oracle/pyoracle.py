@@ -356,12 +356,14 @@ class RefTimer:
     def __init__(self, path: str = REF_TIME_SO):
         self.lib = C.CDLL(path)
         self.lib.ref_time_pairs.argtypes = [C.c_int, C.c_ulonglong, C.c_int, _p, _p, _p, _p, _p, _p, C.c_longlong,
-                                            _p, C.c_int, _p, _p]
+                                            _p, C.c_int, C.c_int, _p, _p]
 
-    def time_pairs(self, K, meshes, quat, pos, pairs, threads=1, mem_bytes=(1 << 64) - 1):
-        """Seconds for one simulation step of the reference over `pairs`:
-        per pair, pose + refit of both meshes and the tandem traversal with
-        contact generation (trees set up untimed on the rest positions)."""
+    def time_pairs(self, K, meshes, quat, pos, pairs, threads=1, mem_bytes=(1 << 64) - 1, repeats=1):
+        """Seconds for simulation steps of the reference over `pairs`: per
+        pair, pose + refit of both meshes and the tandem traversal with
+        contact generation (trees set up once, untimed, on the rest
+        positions).  Returns (seconds of one step, contacts) for repeats == 1,
+        else (list of per-step seconds, contacts of the last step)."""
         n = len(meshes)
         v_off = np.zeros(n + 1, np.int64)
         t_off = np.zeros(n + 1, np.int64)
@@ -372,11 +374,11 @@ class RefTimer:
         tets = _c(np.concatenate([m.tets for m in meshes], axis=0), np.uint32)
         quat, pos = _c(quat, np.float32), _c(pos, np.float32)
         pairs = _c(pairs, np.uint32)
-        sec = C.c_double()
+        sec = np.zeros(max(int(repeats), 1), np.float64)
         cont = C.c_longlong()
         rc = self.lib.ref_time_pairs(K, C.c_ulonglong(mem_bytes), n, _ptr(v_off), _ptr(xyz), _ptr(quat), _ptr(pos),
-                                     _ptr(t_off), _ptr(tets), pairs.shape[0], _ptr(pairs), threads, C.byref(sec),
-                                     C.byref(cont))
+                                     _ptr(t_off), _ptr(tets), pairs.shape[0], _ptr(pairs), threads, len(sec),
+                                     _ptr(sec), C.byref(cont))
         if rc != 0:
             raise RuntimeError(f"ref_time_pairs failed: {rc}")
-        return sec.value, cont.value
+        return (float(sec[0]) if repeats == 1 else [float(x) for x in sec]), cont.value

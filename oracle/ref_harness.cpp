@@ -408,7 +408,7 @@ static int contacts_pairs_t(float const* xyzA, unsigned const* tetsA, unsigned c
 template <size_t K>
 static int time_pairs_k(unsigned long long mem_bytes, int n_meshes, long long const* v_off, float const* xyz,
                         float const* quat, float const* pos, long long const* t_off, unsigned const* tets,
-                        long long n_pairs, unsigned const* pairs, int threads, double* out_seconds,
+                        long long n_pairs, unsigned const* pairs, int threads, int repeats, double* out_seconds,
                         long long* out_contacts) {
   typedef float T;
   typedef tiny::MathTypes<T>::vector3_type V;
@@ -416,16 +416,28 @@ static int time_pairs_k(unsigned long long mem_bytes, int n_meshes, long long co
   std::vector<kdop::Tree<T, K>*> trees(n_meshes, (kdop::Tree<T, K>*)0);
   std::vector<char> used(n_meshes, 0);
   for (long long p = 0; p < n_pairs; ++p) used[pairs[2 * p]] = used[pairs[2 * p + 1]] = 1;
-  for (int m = 0; m < n_meshes; ++m) {
-    if (!used[m]) continue;
-    int nv = (int)(v_off[m + 1] - v_off[m]);
-    int nt = (int)(t_off[m + 1] - t_off[m]);
-    std::vector<unsigned> lt(tets + 4 * t_off[m], tets + 4 * t_off[m + 1]);
-    meshes[m] = new Mesh<T>();
-    trees[m] = new kdop::Tree<T, K>();
-    setup_mesh<T, K>(nv, xyz + 3 * v_off[m], nt, lt.data(), 1, mem_bytes, *meshes[m], *trees[m]);
-  }
   if (threads < 1) threads = 1;
+  // untimed set-up (reorder, surface map, make_tree on the rest positions), meshes in parallel
+  {
+    std::atomic<int> nm(0);
+    auto setup = [&]() {
+      for (;;) {
+        int m = nm.fetch_add(1);
+        if (m >= n_meshes) break;
+        if (!used[m]) continue;
+        int nv = (int)(v_off[m + 1] - v_off[m]);
+        int nt = (int)(t_off[m + 1] - t_off[m]);
+        std::vector<unsigned> lt(tets + 4 * t_off[m], tets + 4 * t_off[m + 1]);
+        meshes[m] = new Mesh<T>();
+        trees[m] = new kdop::Tree<T, K>();
+        setup_mesh<T, K>(nv, xyz + 3 * v_off[m], nt, lt.data(), 1, mem_bytes, *meshes[m], *trees[m]);
+      }
+    };
+    int ns = (int)std::max(1u, std::thread::hardware_concurrency());
+    std::vector<std::thread> th;
+    for (int i = 0; i < ns; ++i) th.push_back(std::thread(setup));
+    for (size_t i = 0; i < th.size(); ++i) th[i].join();
+  }
   std::vector<long long> contacts(threads, 0);
   std::atomic<long long> next(0);
   auto worker = [&](int tid) {
@@ -447,16 +459,21 @@ static int time_pairs_k(unsigned long long mem_bytes, int n_meshes, long long co
       contacts[tid] += (long long)cb.rows.size() / 7;
     }
   };
-  auto t0 = std::chrono::steady_clock::now();
-  if (threads == 1) {
-    worker(0);
-  } else {
-    std::vector<std::thread> th;
-    for (int i = 0; i < threads; ++i) th.push_back(std::thread(worker, i));
-    for (size_t i = 0; i < th.size(); ++i) th[i].join();
+  // `repeats` timed simulation steps over all pairs
+  for (int r = 0; r < std::max(repeats, 1); ++r) {
+    next = 0;
+    for (int i = 0; i < threads; ++i) contacts[i] = 0;
+    auto t0 = std::chrono::steady_clock::now();
+    if (threads == 1) {
+      worker(0);
+    } else {
+      std::vector<std::thread> th;
+      for (int i = 0; i < threads; ++i) th.push_back(std::thread(worker, i));
+      for (size_t i = 0; i < th.size(); ++i) th[i].join();
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    out_seconds[r] = std::chrono::duration<double>(t1 - t0).count();
   }
-  auto t1 = std::chrono::steady_clock::now();
-  *out_seconds = std::chrono::duration<double>(t1 - t0).count();
   long long c = 0;
   for (int i = 0; i < threads; ++i) c += contacts[i];
   *out_contacts = c;
@@ -573,12 +590,12 @@ int ref_traverse(int K, unsigned long long mem_bytes, int reorder, int nvA, floa
 
 int ref_time_pairs(int K, unsigned long long mem_bytes, int n_meshes, long long const* v_off, float const* xyz,
                    float const* quat, float const* pos, long long const* t_off, unsigned const* tets,
-                   long long n_pairs, unsigned const* pairs, int threads, double* out_seconds,
+                   long long n_pairs, unsigned const* pairs, int threads, int repeats, double* out_seconds,
                    long long* out_contacts) {
 #define REFH_TP(KK)                                                                                  \
   case KK:                                                                                           \
     return refh::time_pairs_k<KK>(mem_bytes, n_meshes, v_off, xyz, quat, pos, t_off, tets, n_pairs,  \
-                                  pairs, threads, out_seconds, out_contacts);
+                                  pairs, threads, repeats, out_seconds, out_contacts);
   switch (K) {
     REFH_TP(6) REFH_TP(8) REFH_TP(12) REFH_TP(14) REFH_TP(18) REFH_TP(20) REFH_TP(26)
   }
