@@ -437,7 +437,11 @@ def run_cuda(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "traverse_kernel (batched, one persistent launch)",
-                         "launch_ms": trav_ms, "algorithmic_bytes_per_launch": alg_bytes},
+                         "launch_ms": trav_ms, "algorithmic_bytes_per_launch": alg_bytes,
+                         # DRAM bytes the launch really moves (ncu) over its live duration: the
+                         # algorithmic bytes are mostly served by L1/L2 (records reused per test)
+                         "dram_gbs": (traffic / (trav_ms * 1e-3) / 1e9) if traffic else None,
+                         "dram_frac": (traffic / (trav_ms * 1e-3) / 1e9 / peak) if traffic else None},
             "plain": plain,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
