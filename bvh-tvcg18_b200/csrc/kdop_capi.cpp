@@ -775,6 +775,29 @@ int kdop_traverse(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   return KDOP_OK;
 }
 
+int kdop_traverse_shard(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int memory,
+                        const kdop_traverse_opts* opts, int rank, int n_ranks, int64_t frontier_min) {
+  if (!s || n_pairs < 0 || (n_pairs > 0 && !pairs) || n_ranks < 1 || rank < 0 || rank >= n_ranks ||
+      frontier_min < 1 || frontier_min > ((int64_t)1 << 26))
+    return s ? fail(s->ctx, KDOP_ERR_INVALID, "bad shard arguments") : KDOP_ERR_INVALID;
+  if (n_pairs >= (int64_t)0x7FFFFFFF) return fail(s->ctx, KDOP_ERR_INVALID, "too many pairs");
+  cudaSetDevice(s->ctx->device);
+  kdop::TravParams p;
+  int mode = 0;
+  if (kdop_resolve_traverse_opts(s, opts, p, mode) != KDOP_OK || mode != KDOP_TRAVERSE_BATCHED)
+    return fail(s->ctx, KDOP_ERR_INVALID, "bad traversal options (shards are batched)");
+  int rc = upload_pairs(s, n_pairs, pairs, memory);
+  if (rc != KDOP_OK) return rc;
+  int64_t ne = 0;
+  KDOP_CUDA(s->ctx, kdop::launch_traverse_shard(s, n_pairs, s->pairs, p, rank, n_ranks, frontier_min, &ne));
+  s->traversed = true;
+  s->contacted = false;
+  s->last_pairs = n_pairs;
+  s->last_mode = mode;
+  s->last_params = p;
+  return KDOP_OK;
+}
+
 int kdop_get_stats(kdop_scene* s, kdop_stats* st) {
   if (!s || !st) return KDOP_ERR_INVALID;
   cudaSetDevice(s->ctx->device);

@@ -31,9 +31,11 @@
 //     every wait is bounded by a time limit after which the kernel records
 //     DEV_ERR_TIMEOUT and returns (no unbounded spin).
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 
 #include "kdop_device.cuh"
+#include "kdop_sort.h"
 
 namespace kdop {
 
@@ -57,6 +59,7 @@ struct TravArgs {
   long long timeout_ns;
   unsigned n_meshes;
   const uint32_t* __restrict__ order;  // root pair i -> pair index (NULL: identity)
+  const uint4* __restrict__ entries;   // when set: initial work = these deque entries (A, B, pair)
 };
 
 // Device buffers one traversal works in: pairs (input), candidates (output),
@@ -64,6 +67,7 @@ struct TravArgs {
 struct TravBuffers {
   const uint2* pairs;
   const uint32_t* order;  // processing order of the pairs, or NULL
+  const uint4* entries = nullptr;  // initial deque entries instead of root pairs (n_init of them)
   uint32_t* cand;  // 3 * cand_cap: A tets | B tets | pair ids
   int64_t cand_cap;
   uint4* q_items;
@@ -236,7 +240,14 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
           int n = (int)min((unsigned)a.init_chunk, n_init - base);
           release += n;
           have = true;
-          if (lane < n) {
+          if (lane < n && a.entries) {
+            // a pending node pair of a frontier (its tests are counted already)
+            const uint4 e = a.entries[base + lane];
+            pushA[0] = e.x;
+            pushB[0] = e.y;
+            slotP[0] = e.z;
+            push_mask = 1;
+          } else if (lane < n) {
             // root test (kdop_tandem_traversal.h:164), then the traversal's own
             // test of the root pair (:42), both counted as the reference does.
             uint32_t pid = pair_base + base + lane;
@@ -590,6 +601,7 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
   a.root = s->root_dev;
   a.pairs = b.pairs;
   a.order = b.order;
+  a.entries = b.entries;
   a.candA = b.cand;
   a.candB = b.cand + b.cand_cap;
   a.candP = b.cand + 2 * b.cand_cap;
@@ -604,7 +616,12 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
   a.donate_min = p.donate_min;
   a.surface_filter = p.surface_filter;
   a.timeout_ns = p.timeout_ns;
-  if (!plain) {
+  if (b.entries) {
+    // seeded by a frontier: its tests and leaf pairs are in the totals already
+    trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)n_pairs, 0u, 0, p.stuck_work);
+    traverse_kernel<K, C, S><<<grid, threads, smem, st>>>(a);
+    s->ctx->launches += 2;
+  } else if (!plain) {
     // waves of wave_pairs root pairs (largest first), or all at once
     int64_t wave = p.wave_pairs > 0 ? p.wave_pairs : n_pairs;
     if (wave < 1) wave = 1;
@@ -671,6 +688,243 @@ cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, 
   b.q_cap = s->queue_cap;
   b.ctl = s->ctl;
   return traverse_buffers(s, n_pairs, b, p, plain);
+}
+
+// ---- frontier-seeded and sharded traversal ----------------------------------
+// The node-pair tree is expanded breadth first, one launch per level, until
+// enough pairs are pending; every test and leaf pair of that expansion is the
+// reference's own (the same rule, in breadth-first order).  The pending pairs
+// are sorted (a deterministic list on every rank) and dealt round-robin to the
+// shards; each shard's persistent traversal starts from its share.
+namespace {
+
+template <int K>
+__device__ void frontier_emit(const TravArgs& a, uint32_t wa, uint32_t wb, uint32_t pid) {
+  unsigned at = atomicAdd(&a.ctl->n_cand, 1u);
+  if (at < a.cand_cap) {
+    a.candA[at] = leaf_tet<K>(a.nodes, wa);
+    a.candB[at] = leaf_tet<K>(a.nodes, wb);
+    a.candP[at] = pid;
+  }
+}
+
+__device__ void frontier_push(uint4* out, unsigned* count, unsigned cap, uint32_t wa, uint32_t wb, uint32_t pid,
+                              unsigned* error) {
+  unsigned at = atomicAdd(count, 1u);
+  if (at < cap)
+    out[at] = make_uint4(wa, wb, pid, 0u);
+  else
+    atomicOr(error, DEV_ERR_QUEUE_FULL);
+}
+
+// root test of each mesh pair (kdop_tandem_traversal.h:164, then :42)
+template <int K>
+__global__ void frontier_root_kernel(TravArgs a, unsigned n_pairs, uint4* out, unsigned* count, unsigned cap) {
+  unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_pairs) return;
+  uint2 mp = a.pairs[p];
+  if (mp.x >= a.n_meshes || mp.y >= a.n_meshes) {
+    atomicOr(&a.ctl->error, DEV_ERR_BAD_INDEX);
+    return;
+  }
+  uint32_t ra = a.root[mp.x], rb = a.root[mp.y];
+  if (ra == NO_NODE || rb == NO_NODE) return;
+  uint32_t wa, wb;
+  bool ov = node_overlap<K>(a.nodes, ra, rb, wa, wb);
+  atomicAdd(&a.ctl->tests, ov ? 2ull : 1ull);
+  if (!ov) return;
+  if (wa & wb & LEAF_BIT) {
+    atomicAdd(&a.ctl->leaf_overlaps, 1ull);
+    if (!a.surface_filter || (wa & wb & SURF_BIT)) frontier_emit<K>(a, wa, wb, p);
+  } else {
+    frontier_push(out, count, cap, wa, wb, p, &a.ctl->error);
+  }
+}
+
+// one level: every pending pair's child pairs
+template <int K>
+__global__ void frontier_level_kernel(TravArgs a, const uint4* __restrict__ in, unsigned n_in, uint4* out,
+                                      unsigned* count, unsigned cap) {
+  unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_in) return;
+  uint4 e = in[i];
+  uint32_t A[2], B[2];
+  int na = 2, nb = 2;
+  if (e.x & LEAF_BIT) {
+    A[0] = e.x & NODE_MASK;
+    na = 1;
+  } else {
+    A[0] = e.x;
+    A[1] = e.x + 1;
+  }
+  if (e.y & LEAF_BIT) {
+    B[0] = e.y & NODE_MASK;
+    nb = 1;
+  } else {
+    B[0] = e.y;
+    B[1] = e.y + 1;
+  }
+  unsigned long long lo = 0;
+  for (int x = 0; x < na; ++x)
+    for (int y = 0; y < nb; ++y) {
+      uint32_t wa, wb;
+      if (!node_overlap<K>(a.nodes, A[x], B[y], wa, wb)) continue;
+      if (wa & wb & LEAF_BIT) {
+        ++lo;
+        if (!a.surface_filter || (wa & wb & SURF_BIT)) frontier_emit<K>(a, wa, wb, e.z);
+      } else {
+        frontier_push(out, count, cap, wa, wb, e.z, &a.ctl->error);
+      }
+    }
+  atomicAdd(&a.ctl->tests, (unsigned long long)(na * nb));
+  if (lo) atomicAdd(&a.ctl->leaf_overlaps, lo);
+}
+
+__global__ void entry_keys_kernel(const uint4* __restrict__ f, unsigned n, uint64_t* keys, uint32_t* vals,
+                                  int by_pair) {
+  unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (by_pair) {
+    keys[i] = f[vals[i]].z;
+  } else {
+    uint4 e = f[i];
+    keys[i] = ((uint64_t)e.x << 32) | e.y;
+    vals[i] = i;
+  }
+}
+
+// this shard's entries: sorted positions rank, rank + n_ranks, ...
+__global__ void deal_kernel(const uint4* __restrict__ f, const uint32_t* __restrict__ order, unsigned n, int rank,
+                            int n_ranks, uint4* mine) {
+  unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned src = (unsigned)rank + j * (unsigned)n_ranks;
+  if (src < n) mine[j] = f[order[src]];
+}
+
+__global__ void clear_totals_kernel(TravCtl* c) {
+  if (threadIdx.x == 0) {
+    c->tests = 0;
+    c->leaf_overlaps = 0;
+    c->n_cand = 0;
+  }
+}
+
+template <int K>
+TravArgs frontier_args(kdop_scene* s, const uint2* pairs, const TravParams& p) {
+  TravArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.nodes = s->nodes;
+  a.surf = s->surf;
+  a.root = s->root_dev;
+  a.pairs = pairs;
+  a.candA = s->cand;
+  a.candB = s->cand + s->cand_cap;
+  a.candP = s->cand + 2 * s->cand_cap;
+  a.cand_cap = (unsigned)s->cand_cap;
+  a.ctl = s->ctl;
+  a.n_meshes = (unsigned)s->n_meshes;
+  a.surface_filter = p.surface_filter;
+  return a;
+}
+
+template <int K>
+cudaError_t shard_impl(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int rank,
+                       int n_ranks, int64_t frontier_min, int64_t* n_entries) {
+  cudaStream_t st = s->ctx->stream;
+  const int64_t fmin = std::max<int64_t>(frontier_min, 1);
+  const int64_t cap = std::max<int64_t>(8 * fmin, n_pairs) + 1024;
+  // work: two frontiers, their count, the sort (keys 2 cap, vals 2 cap, scratch), this shard's entries
+  size_t bytes = 0;
+  auto take = [&](size_t b) {
+    size_t o = bytes;
+    bytes += (b + 255) & ~(size_t)255;
+    return o;
+  };
+  const size_t o_f0 = take((size_t)cap * 16), o_f1 = take((size_t)cap * 16), o_cnt = take(16),
+               o_k = take((size_t)cap * 8), o_kt = take((size_t)cap * 8), o_v = take((size_t)cap * 4),
+               o_vt = take((size_t)cap * 4), o_sc = take(radix_scratch_words(cap) * 4),
+               o_mine = take((size_t)cap * 16);
+  char* w = nullptr;
+  cudaError_t e = cudaMalloc((void**)&w, bytes);
+  if (e != cudaSuccess) return e;
+  uint4* F[2] = {reinterpret_cast<uint4*>(w + o_f0), reinterpret_cast<uint4*>(w + o_f1)};
+  unsigned* cnt = reinterpret_cast<unsigned*>(w + o_cnt);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(w + o_k);
+  uint64_t* ktmp = reinterpret_cast<uint64_t*>(w + o_kt);
+  uint32_t* vals = reinterpret_cast<uint32_t*>(w + o_v);
+  uint32_t* vtmp = reinterpret_cast<uint32_t*>(w + o_vt);
+  uint32_t* scratch = reinterpret_cast<uint32_t*>(w + o_sc);
+  uint4* mine = reinterpret_cast<uint4*>(w + o_mine);
+  TravArgs a = frontier_args<K>(s, pairs, p);
+  int cur = 0;
+  unsigned n = 0;
+  do {
+    trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, 0u, 0u, 1, 0);  // totals and queue state to zero
+    if ((e = cudaMemsetAsync(cnt, 0, 4, st)) != cudaSuccess) break;
+    if (n_pairs > 0)
+      frontier_root_kernel<K><<<(unsigned)((n_pairs + 255) / 256), 256, 0, st>>>(a, (unsigned)n_pairs, F[0], cnt,
+                                                                                  (unsigned)cap);
+    s->ctx->launches += 2;
+    for (int level = 0; level < 48; ++level) {
+      if ((e = cudaMemcpyAsync(&n, cnt, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) break;
+      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) break;
+      if (n > (unsigned)cap) n = (unsigned)cap;  // overflow is flagged in the control block
+      if (n == 0 || (int64_t)n >= fmin || 4 * (int64_t)n > cap) break;
+      if ((e = cudaMemsetAsync(cnt, 0, 4, st)) != cudaSuccess) break;
+      frontier_level_kernel<K><<<(n + 255) / 256, 256, 0, st>>>(a, F[cur], n, F[1 - cur], cnt, (unsigned)cap);
+      s->ctx->launches++;
+      cur = 1 - cur;
+    }
+    if (e != cudaSuccess) break;
+    // deterministic order: by (A, B), then by pair
+    if (n > 0) {
+      const unsigned g = (n + 255) / 256;
+      entry_keys_kernel<<<g, 256, 0, st>>>(F[cur], n, keys, vals, 0);
+      if ((e = radix_sort_pairs(keys, vals, ktmp, vtmp, n, scratch, st)) != cudaSuccess) break;
+      entry_keys_kernel<<<g, 256, 0, st>>>(F[cur], n, keys, vals, 1);
+      if ((e = radix_sort_pairs(keys, vals, ktmp, vtmp, n, scratch, st)) != cudaSuccess) break;
+      deal_kernel<<<g, 256, 0, st>>>(F[cur], vals, n, rank, n_ranks, mine);
+      s->ctx->launches += 3;
+    }
+    // the expansion's tests and leaf pairs belong to shard 0
+    if (rank != 0) {
+      clear_totals_kernel<<<1, 32, 0, st>>>(s->ctl);
+      s->ctx->launches++;
+    }
+    const int64_t m = n > (unsigned)rank ? ((int64_t)n - rank + n_ranks - 1) / n_ranks : 0;
+    *n_entries = m;
+    TravBuffers b;
+    b.pairs = pairs;
+    b.order = nullptr;
+    b.entries = mine;
+    b.cand = s->cand;
+    b.cand_cap = s->cand_cap;
+    b.q_items = s->q_items;
+    b.q_tags = s->q_tags;
+    b.q_cap = s->queue_cap;
+    b.ctl = s->ctl;
+    e = traverse_group<K>(s, m, b, p, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  } while (0);
+  cudaStreamSynchronize(st);
+  cudaFree(w);
+  return e;
+}
+
+}  // namespace
+
+cudaError_t launch_traverse_shard(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int rank,
+                                  int n_ranks, int64_t frontier_min, int64_t* n_entries) {
+  switch (s->K) {
+    case 6: return shard_impl<6>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+    case 8: return shard_impl<8>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+    case 12: return shard_impl<12>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+    case 14: return shard_impl<14>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+    case 18: return shard_impl<18>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+    case 20: return shard_impl<20>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+    case 26: return shard_impl<26>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+  }
+  return cudaErrorInvalidValue;
 }
 
 }  // namespace kdop

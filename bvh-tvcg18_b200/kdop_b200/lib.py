@@ -114,6 +114,7 @@ def load_library():
         "kdop_read_candidates": ([vp, vp, i64, C.POINTER(i64)], i32),
         "kdop_contacts": ([vp], i32),
         "kdop_sort_results": ([vp], i32),
+        "kdop_traverse_shard": ([vp, i64, vp, i32, C.POINTER(TraverseOpts), i32, i32, i64], i32),
         "kdop_read_contacts": ([vp, vp, i64, C.POINTER(i64)], i32),
         "kdop_contacts_adjoint": ([vp, vp, vp, vp, i32], i32),
         "kdop_set_motion": ([vp, vp, vp, C.c_float, i32], i32),
@@ -296,6 +297,17 @@ class DeviceScene:
         self.pairs = p
         self.ctx._check(self.lib.kdop_traverse(self.h, n, _ptr(p), _mem(p), C.byref(opts) if opts else None),
                         "kdop_traverse")
+
+    def traverse_shard(self, pairs, rank: int, n_ranks: int, frontier_min: int = 16384,
+                       opts: Optional[TraverseOpts] = None):
+        """Shard `rank` of `n_ranks` of the traversal (frontier-seeded): the
+        shards' candidates and test counts together equal traverse()'s."""
+        p = _arg(pairs, np.uint32)
+        n = p.shape[0] if p.ndim == 2 else p.size // 2
+        self.pairs = p
+        self.ctx._check(self.lib.kdop_traverse_shard(self.h, n, _ptr(p), _mem(p), C.byref(opts) if opts else None,
+                                                     int(rank), int(n_ranks), int(frontier_min)),
+                        "kdop_traverse_shard")
 
     def stats(self, check: bool = True) -> Stats:
         st = Stats()

@@ -201,6 +201,21 @@ typedef struct {
  * defaults. */
 int kdop_traverse(kdop_scene* scene, int64_t n_pairs, const uint32_t* pairs, int memory,
                   const kdop_traverse_opts* opts);
+
+/* One shard of a traversal, for splitting few large pairs (one huge pair
+ * included) over ranks or GPUs.  The node-pair tree of the given pairs is
+ * expanded breadth first until at least frontier_min node pairs are pending
+ * (the tests and leaf pairs of that expansion count on shard 0); the pending
+ * pairs are sorted -- the same list on every rank -- and dealt round-robin,
+ * and this call traverses shard `rank` of `n_ranks` from its share.  The
+ * shards' candidate rows and test counts together equal kdop_traverse's
+ * (each candidate on exactly one shard); kdop_contacts etc. then work on the
+ * shard's rows.  With n_ranks = 1 it is kdop_traverse seeded by the frontier.
+ * Batched mode only.  Synchronises.  The sharded (multi-GPU) use of the
+ * reference's single-pair traversal (kdop_tandem_traversal.h:161-196) has no
+ * counterpart there. */
+int kdop_traverse_shard(kdop_scene* scene, int64_t n_pairs, const uint32_t* pairs, int memory,
+                        const kdop_traverse_opts* opts, int rank, int n_ranks, int64_t frontier_min);
 /* Synchronises and reads the counters of the last traversal/contacts.
  * Returns KDOP_ERR_CAPACITY when candidates, contacts or the work queue
  * overflowed (stats then hold the required sizes), KDOP_ERR_TIMEOUT when a
