@@ -72,6 +72,8 @@ struct kdop_scene_ext {
   int64_t stage_n = 0;
   void* sort_work = nullptr;  // kdop_sort_results scratch
   size_t sort_work_bytes = 0;
+  void* shard_work = nullptr;  // kdop_traverse_shard scratch
+  size_t shard_work_bytes = 0;
   std::vector<uint32_t> pairs_host;  // last traversed mesh pairs
   std::vector<uint32_t> order_host;  // their order of processing
   int64_t graph_kernels = 0;
@@ -228,6 +230,9 @@ static void scene_free(kdop_scene* s) {
   if (x->sort_work) cudaFree(x->sort_work);
   x->sort_work = nullptr;
   x->sort_work_bytes = 0;
+  if (x->shard_work) cudaFree(x->shard_work);
+  x->shard_work = nullptr;
+  x->shard_work_bytes = 0;
 }
 
 // A captured graph holds the buffer addresses of its capture: any
@@ -789,7 +794,12 @@ int kdop_traverse_shard(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, i
   int rc = upload_pairs(s, n_pairs, pairs, memory);
   if (rc != KDOP_OK) return rc;
   int64_t ne = 0;
-  KDOP_CUDA(s->ctx, kdop::launch_traverse_shard(s, n_pairs, s->pairs, p, rank, n_ranks, frontier_min, &ne));
+  kdop_scene_ext* x = ext(s);
+  size_t before = x->shard_work_bytes;
+  cudaError_t e = kdop::launch_traverse_shard(s, n_pairs, s->pairs, p, rank, n_ranks, frontier_min, &x->shard_work,
+                                              &x->shard_work_bytes, &ne);
+  s->device_bytes += (int64_t)x->shard_work_bytes - (int64_t)before;
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "kdop_traverse_shard");
   s->traversed = true;
   s->contacted = false;
   s->last_pairs = n_pairs;

@@ -200,10 +200,12 @@ void surface_map(int64_t n_tets, const uint32_t* tets, uint8_t* surf);
 cudaError_t launch_write_topology(kdop_scene* s, const uint32_t* topo_dev);
 cudaError_t launch_refit(kdop_scene* s, int mode);
 cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int plain);
-// Frontier-seeded traversal of shard `rank` of `n_ranks` (synchronises);
-// *n_entries = frontier pairs this shard started from.
+// Frontier-seeded traversal of shard `rank` of `n_ranks` (synchronises once,
+// for the frontier's size); *work / *work_bytes: the scene's scratch for it,
+// grown here; *n_entries = frontier pairs this shard started from.
 cudaError_t launch_traverse_shard(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int rank,
-                                  int n_ranks, int64_t frontier_min, int64_t* n_entries);
+                                  int n_ranks, int64_t frontier_min, void** work, size_t* work_bytes,
+                                  int64_t* n_entries);
 cudaError_t launch_contacts(kdop_scene* s);
 cudaError_t launch_adjoint(kdop_scene* s, const float* dd, const float* dn, float* grad);
 cudaError_t launch_motion(kdop_scene* s);

@@ -720,6 +720,7 @@ __device__ void frontier_push(uint4* out, unsigned* count, unsigned cap, uint32_
 // root test of each mesh pair (kdop_tandem_traversal.h:164, then :42)
 template <int K>
 __global__ void frontier_root_kernel(TravArgs a, unsigned n_pairs, uint4* out, unsigned* count, unsigned cap) {
+  // count: level 0's count (the frontier state's first word)
   unsigned p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n_pairs) return;
   uint2 mp = a.pairs[p];
@@ -741,12 +742,30 @@ __global__ void frontier_root_kernel(TravArgs a, unsigned n_pairs, uint4* out, u
   }
 }
 
-// one level: every pending pair's child pairs
+// Frontier state: level counts fs[0 .. kMaxLevels], then the frozen flag,
+// the final level and the final count.
+constexpr int kMaxLevels = 20;
+constexpr int FS_FROZEN = kMaxLevels + 1, FS_LEVEL = kMaxLevels + 2, FS_COUNT = kMaxLevels + 3, FS_WORDS = 32;
+
+// one level: every pending pair's child pairs.  The level stops the expansion
+// (freezes) when its input is empty, large enough, or could overflow the
+// next buffer; all later levels then do nothing.  Every thread reads the
+// same counts, so they all take the same decision.
 template <int K>
-__global__ void frontier_level_kernel(TravArgs a, const uint4* __restrict__ in, unsigned n_in, uint4* out,
-                                      unsigned* count, unsigned cap) {
-  unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_in) return;
+__global__ void frontier_level_kernel(TravArgs a, int level, const uint4* __restrict__ in, uint4* out, unsigned* fs,
+                                      unsigned cap, unsigned fmin) {
+  if (fs[FS_FROZEN]) return;
+  const unsigned n_in = min(fs[level], cap);
+  if (n_in == 0 || n_in >= fmin || 4ull * n_in > cap) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      fs[FS_FROZEN] = 1u;
+      fs[FS_LEVEL] = (unsigned)level;
+      fs[FS_COUNT] = n_in;
+    }
+    return;
+  }
+  unsigned* count = fs + level + 1;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n_in; i += gridDim.x * blockDim.x) {
   uint4 e = in[i];
   uint32_t A[2], B[2];
   int na = 2, nb = 2;
@@ -778,6 +797,15 @@ __global__ void frontier_level_kernel(TravArgs a, const uint4* __restrict__ in, 
     }
   atomicAdd(&a.ctl->tests, (unsigned long long)(na * nb));
   if (lo) atomicAdd(&a.ctl->leaf_overlaps, lo);
+  }
+}
+
+__global__ void frontier_final_kernel(unsigned* fs, unsigned cap) {
+  if (threadIdx.x == 0 && !fs[FS_FROZEN]) {
+    fs[FS_FROZEN] = 1u;
+    fs[FS_LEVEL] = kMaxLevels;
+    fs[FS_COUNT] = min(fs[kMaxLevels], cap);
+  }
 }
 
 __global__ void entry_keys_kernel(const uint4* __restrict__ f, unsigned n, uint64_t* keys, uint32_t* vals,
@@ -827,102 +855,115 @@ TravArgs frontier_args(kdop_scene* s, const uint2* pairs, const TravParams& p) {
   return a;
 }
 
+// Work buffer of a sharded traversal: frontier state, two frontiers, the
+// sort (keys, values, scratch), this shard's entries; 256-byte regions.
+struct ShardWork {
+  size_t fs, f0, f1, k, kt, v, vt, sc, mine, total;
+  explicit ShardWork(int64_t cap) {
+    size_t at = 0;
+    auto take = [&](size_t b) {
+      size_t o = at;
+      at += (b + 255) & ~(size_t)255;
+      return o;
+    };
+    fs = take(FS_WORDS * 4);
+    f0 = take((size_t)cap * 16);
+    f1 = take((size_t)cap * 16);
+    k = take((size_t)cap * 8);
+    kt = take((size_t)cap * 8);
+    v = take((size_t)cap * 4);
+    vt = take((size_t)cap * 4);
+    sc = take(radix_scratch_words(cap) * 4);
+    mine = take((size_t)cap * 16);
+    total = at;
+  }
+};
+
 template <int K>
 cudaError_t shard_impl(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int rank,
-                       int n_ranks, int64_t frontier_min, int64_t* n_entries) {
+                       int n_ranks, int64_t frontier_min, char* w, int64_t cap, int64_t* n_entries) {
   cudaStream_t st = s->ctx->stream;
-  const int64_t fmin = std::max<int64_t>(frontier_min, 1);
-  const int64_t cap = std::max<int64_t>(8 * fmin, n_pairs) + 1024;
-  // work: two frontiers, their count, the sort (keys 2 cap, vals 2 cap, scratch), this shard's entries
-  size_t bytes = 0;
-  auto take = [&](size_t b) {
-    size_t o = bytes;
-    bytes += (b + 255) & ~(size_t)255;
-    return o;
-  };
-  const size_t o_f0 = take((size_t)cap * 16), o_f1 = take((size_t)cap * 16), o_cnt = take(16),
-               o_k = take((size_t)cap * 8), o_kt = take((size_t)cap * 8), o_v = take((size_t)cap * 4),
-               o_vt = take((size_t)cap * 4), o_sc = take(radix_scratch_words(cap) * 4),
-               o_mine = take((size_t)cap * 16);
-  char* w = nullptr;
-  cudaError_t e = cudaMalloc((void**)&w, bytes);
-  if (e != cudaSuccess) return e;
-  uint4* F[2] = {reinterpret_cast<uint4*>(w + o_f0), reinterpret_cast<uint4*>(w + o_f1)};
-  unsigned* cnt = reinterpret_cast<unsigned*>(w + o_cnt);
-  uint64_t* keys = reinterpret_cast<uint64_t*>(w + o_k);
-  uint64_t* ktmp = reinterpret_cast<uint64_t*>(w + o_kt);
-  uint32_t* vals = reinterpret_cast<uint32_t*>(w + o_v);
-  uint32_t* vtmp = reinterpret_cast<uint32_t*>(w + o_vt);
-  uint32_t* scratch = reinterpret_cast<uint32_t*>(w + o_sc);
-  uint4* mine = reinterpret_cast<uint4*>(w + o_mine);
+  ShardWork L(cap);
+  unsigned* fs = reinterpret_cast<unsigned*>(w + L.fs);
+  uint4* F[2] = {reinterpret_cast<uint4*>(w + L.f0), reinterpret_cast<uint4*>(w + L.f1)};
+  uint64_t* keys = reinterpret_cast<uint64_t*>(w + L.k);
+  uint64_t* ktmp = reinterpret_cast<uint64_t*>(w + L.kt);
+  uint32_t* vals = reinterpret_cast<uint32_t*>(w + L.v);
+  uint32_t* vtmp = reinterpret_cast<uint32_t*>(w + L.vt);
+  uint32_t* scratch = reinterpret_cast<uint32_t*>(w + L.sc);
+  uint4* mine = reinterpret_cast<uint4*>(w + L.mine);
   TravArgs a = frontier_args<K>(s, pairs, p);
-  int cur = 0;
-  unsigned n = 0;
-  do {
-    trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, 0u, 0u, 1, 0);  // totals and queue state to zero
-    if ((e = cudaMemsetAsync(cnt, 0, 4, st)) != cudaSuccess) break;
-    if (n_pairs > 0)
-      frontier_root_kernel<K><<<(unsigned)((n_pairs + 255) / 256), 256, 0, st>>>(a, (unsigned)n_pairs, F[0], cnt,
-                                                                                  (unsigned)cap);
-    s->ctx->launches += 2;
-    for (int level = 0; level < 48; ++level) {
-      if ((e = cudaMemcpyAsync(&n, cnt, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) break;
-      if ((e = cudaStreamSynchronize(st)) != cudaSuccess) break;
-      if (n > (unsigned)cap) n = (unsigned)cap;  // overflow is flagged in the control block
-      if (n == 0 || (int64_t)n >= fmin || 4 * (int64_t)n > cap) break;
-      if ((e = cudaMemsetAsync(cnt, 0, 4, st)) != cudaSuccess) break;
-      frontier_level_kernel<K><<<(n + 255) / 256, 256, 0, st>>>(a, F[cur], n, F[1 - cur], cnt, (unsigned)cap);
-      s->ctx->launches++;
-      cur = 1 - cur;
-    }
-    if (e != cudaSuccess) break;
-    // deterministic order: by (A, B), then by pair
-    if (n > 0) {
-      const unsigned g = (n + 255) / 256;
-      entry_keys_kernel<<<g, 256, 0, st>>>(F[cur], n, keys, vals, 0);
-      if ((e = radix_sort_pairs(keys, vals, ktmp, vtmp, n, scratch, st)) != cudaSuccess) break;
-      entry_keys_kernel<<<g, 256, 0, st>>>(F[cur], n, keys, vals, 1);
-      if ((e = radix_sort_pairs(keys, vals, ktmp, vtmp, n, scratch, st)) != cudaSuccess) break;
-      deal_kernel<<<g, 256, 0, st>>>(F[cur], vals, n, rank, n_ranks, mine);
-      s->ctx->launches += 3;
-    }
-    // the expansion's tests and leaf pairs belong to shard 0
-    if (rank != 0) {
-      clear_totals_kernel<<<1, 32, 0, st>>>(s->ctl);
-      s->ctx->launches++;
-    }
-    const int64_t m = n > (unsigned)rank ? ((int64_t)n - rank + n_ranks - 1) / n_ranks : 0;
-    *n_entries = m;
-    TravBuffers b;
-    b.pairs = pairs;
-    b.order = nullptr;
-    b.entries = mine;
-    b.cand = s->cand;
-    b.cand_cap = s->cand_cap;
-    b.q_items = s->q_items;
-    b.q_tags = s->q_tags;
-    b.q_cap = s->queue_cap;
-    b.ctl = s->ctl;
-    e = traverse_group<K>(s, m, b, p, 0);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  } while (0);
-  cudaStreamSynchronize(st);
-  cudaFree(w);
-  return e;
+  cudaError_t e;
+  trav_init_kernel<<<1, 32, 0, st>>>(s->ctl, 0u, 0u, 1, 0);  // totals and queue state to zero
+  if ((e = cudaMemsetAsync(fs, 0, FS_WORDS * 4, st)) != cudaSuccess) return e;
+  if (n_pairs > 0)
+    frontier_root_kernel<K><<<(unsigned)((n_pairs + 255) / 256), 256, 0, st>>>(a, (unsigned)n_pairs, F[0], fs,
+                                                                                (unsigned)cap);
+  const unsigned g = (unsigned)std::min<int64_t>((cap / 4 + 255) / 256, 4 * (int64_t)s->ctx->sm_count);
+  for (int level = 0; level < kMaxLevels; ++level)
+    frontier_level_kernel<K><<<g, 256, 0, st>>>(a, level, F[level & 1], F[(level + 1) & 1], fs, (unsigned)cap,
+                                               (unsigned)frontier_min);
+  frontier_final_kernel<<<1, 32, 0, st>>>(fs, (unsigned)cap);
+  s->ctx->launches += 3 + kMaxLevels;
+  unsigned hfs[FS_WORDS];
+  if ((e = cudaMemcpyAsync(hfs, fs, sizeof(hfs), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  const unsigned n = hfs[FS_COUNT];
+  const uint4* fin = F[hfs[FS_LEVEL] & 1];
+  // deterministic order: by (A, B), then by pair
+  if (n > 0) {
+    const unsigned gn = (n + 255) / 256;
+    entry_keys_kernel<<<gn, 256, 0, st>>>(fin, n, keys, vals, 0);
+    if ((e = radix_sort_pairs(keys, vals, ktmp, vtmp, n, scratch, st)) != cudaSuccess) return e;
+    entry_keys_kernel<<<gn, 256, 0, st>>>(fin, n, keys, vals, 1);
+    if ((e = radix_sort_pairs(keys, vals, ktmp, vtmp, n, scratch, st)) != cudaSuccess) return e;
+    deal_kernel<<<gn, 256, 0, st>>>(fin, vals, n, rank, n_ranks, mine);
+    s->ctx->launches += 3;
+  }
+  // the expansion's tests and leaf pairs belong to shard 0
+  if (rank != 0) {
+    clear_totals_kernel<<<1, 32, 0, st>>>(s->ctl);
+    s->ctx->launches++;
+  }
+  const int64_t m = n > (unsigned)rank ? ((int64_t)n - rank + n_ranks - 1) / n_ranks : 0;
+  *n_entries = m;
+  TravBuffers b;
+  b.pairs = pairs;
+  b.order = nullptr;
+  b.entries = mine;
+  b.cand = s->cand;
+  b.cand_cap = s->cand_cap;
+  b.q_items = s->q_items;
+  b.q_tags = s->q_tags;
+  b.q_cap = s->queue_cap;
+  b.ctl = s->ctl;
+  return traverse_group<K>(s, m, b, p, 0);
 }
 
 }  // namespace
 
 cudaError_t launch_traverse_shard(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int rank,
-                                  int n_ranks, int64_t frontier_min, int64_t* n_entries) {
+                                  int n_ranks, int64_t frontier_min, void** work, size_t* work_bytes,
+                                  int64_t* n_entries) {
+  const int64_t cap = std::max<int64_t>(8 * std::max<int64_t>(frontier_min, 1), n_pairs) + 1024;
+  const size_t need = ShardWork(cap).total;
+  if (*work_bytes < need) {
+    if (*work) cudaFree(*work);
+    *work = nullptr;
+    *work_bytes = 0;
+    cudaError_t e = cudaMalloc(work, need);
+    if (e != cudaSuccess) return e;
+    *work_bytes = need;
+  }
+  char* w = static_cast<char*>(*work);
   switch (s->K) {
-    case 6: return shard_impl<6>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
-    case 8: return shard_impl<8>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
-    case 12: return shard_impl<12>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
-    case 14: return shard_impl<14>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
-    case 18: return shard_impl<18>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
-    case 20: return shard_impl<20>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
-    case 26: return shard_impl<26>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, n_entries);
+    case 6: return shard_impl<6>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, w, cap, n_entries);
+    case 8: return shard_impl<8>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, w, cap, n_entries);
+    case 12: return shard_impl<12>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, w, cap, n_entries);
+    case 14: return shard_impl<14>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, w, cap, n_entries);
+    case 18: return shard_impl<18>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, w, cap, n_entries);
+    case 20: return shard_impl<20>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, w, cap, n_entries);
+    case 26: return shard_impl<26>(s, n_pairs, pairs, p, rank, n_ranks, frontier_min, w, cap, n_entries);
   }
   return cudaErrorInvalidValue;
 }
