@@ -54,6 +54,10 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU-baseline sample, seconds")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--opts", default="", help="traversal options key=value,... (skips the autotuner)")
+    ap.add_argument("--shard", action="store_true",
+                    help="strong scaling: every rank takes the same pairs and traverses its shard of their "
+                         "node-pair tree (kdop_traverse_shard); contacts all-gathered to rank 0 each step")
+    ap.add_argument("--frontier", type=int, default=16384, help="--shard: frontier node pairs before dealing")
     return ap.parse_args()
 
 
@@ -254,6 +258,113 @@ def run_reference(args):
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+# ---- CUDA arm, sharded: one workload split over the ranks --------------------------------
+def run_cuda_sharded(args):
+    import torch
+
+    import kdop_b200 as kd
+
+    dist = Dist("nccl")
+    torch.cuda.set_device(dist.local)
+    sc = workload(args, 0)  # the same pairs on every rank
+    ctx = kd.Context(dist.local)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    full = ds.traverse_sync(sc.pairs, contacts=True)
+    ds.reserve(candidates=int(full.n_candidates * 1.2) + 1024, contacts=int(full.n_contacts * 1.2) + 1024,
+               queue=max(full.queue_used * 2, 1 << 20))
+    opts = ds.default_opts()
+    row_bytes = 32
+    cap_rows = int(full.n_contacts * 1.2) + 1024
+    mine = torch.empty(cap_rows * row_bytes, dtype=torch.uint8, device="cuda")
+    gathered = [torch.empty_like(mine) for _ in range(dist.world)]
+    host_rows = torch.empty(cap_rows * row_bytes * dist.world, dtype=torch.uint8).pin_memory()
+
+    def step():
+        # poses in from the host, refit, this rank's shard, contacts, then the
+        # exchange: every rank's rows to rank 0
+        ds.set_poses(sc.quat, sc.pos)
+        ds.refit(kd.REFIT_POSE)
+        ds.traverse_shard(sc.pairs, dist.rank, dist.world, args.frontier, opts)
+        ds.contacts()
+        st = ds.stats()
+        n = ds.read_contacts_into(mine)
+        with torch.cuda.stream(stream):
+            counts = torch.tensor([n], dtype=torch.int64, device="cuda")
+            if dist.pg:
+                all_counts = [torch.empty_like(counts) for _ in range(dist.world)]
+                dist.pg.all_gather(all_counts, counts)
+                dist.pg.all_gather(gathered, mine)
+                cnt = [int(c.item()) for c in all_counts]
+            else:
+                gathered[0].copy_(mine)
+                cnt = [n]
+            if dist.rank == 0:
+                off = 0
+                for r, c in enumerate(cnt):
+                    if c:
+                        host_rows[off: off + c * row_bytes].copy_(gathered[r][: c * row_bytes], non_blocking=True)
+                    off += c * row_bytes
+            stream.synchronize()
+        return st.n_tests, sum(cnt)
+
+    for _ in range(args.warmup):
+        step()
+    ctx.synchronize()
+    dist.barrier()
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    clocks.wait_ready()
+    times, tests, rows = [], 0, 0
+    launches0 = ctx.launches
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        t, rows = step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        tests = t
+    clk = clocks.stop()
+    ms = sum(times) / len(times)
+    ms_max = dist.max(ms)
+    total_tests = dist.sum(tests)
+    dist.barrier()
+    if dist.rank == 0:
+        value = total_tests / (ms_max * 1e-3)
+        node_bytes = ds.info()["node_bytes"]
+        peak, peak_kind = measured_peaks()
+        alg = total_tests * 2 * node_bytes / dist.world
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": sc.name, "pairs": int(len(sc.pairs)), "K": sc.K,
+                       "parallelism": f"node-pair tree sharded over {dist.world} rank(s) from a "
+                                      f"{args.frontier}-pair frontier; contacts all-gathered to rank 0",
+                       "tests_per_step": int(total_tests), "contacts": int(rows),
+                       "step": "poses H2D, refit, traversal shard, contacts, contact all-gather + D2H"},
+            "roofline": {"bound": "hbm", "achieved": alg / (ms_max * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": alg / (ms_max * 1e-3) / 1e9 / peak, "traffic": None, "peak_kind": peak_kind,
+                         "kernel": "whole step per rank (algorithmic bytes of its share of the tests)"},
+            "cpu_baseline": None,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(sc.quat.nbytes + sc.pos.nbytes),
+                    "d2h_bytes_per_step": int(rows * row_bytes)},
+            "gpu_launches": int(ctx.launches - launches0), "clocks": clk,
+        }
+        print(json.dumps(line))
+    # buffers used on the library's stream go before the stream does
+    del mine, gathered, host_rows
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    ds.close()
+    ctx.close()
+    dist.close()
 
 
 # ---- CUDA arm -------------------------------------------------------------------------
@@ -461,7 +572,7 @@ def main():
     if args.impl == "reference":
         run_reference(args)
     else:
-        run_cuda(args)
+        run_cuda_sharded(args) if args.shard else run_cuda(args)
 
 
 if __name__ == "__main__":

@@ -951,7 +951,7 @@ int kdop_read_contacts(kdop_scene* s, kdop_contact* rows, int64_t cap, int64_t* 
   *n_rows = n;
   if (n > cap) return fail(s->ctx, KDOP_ERR_CAPACITY, "contact read buffer too small");
   if (n == 0) return KDOP_OK;
-  KDOP_CUDA(s->ctx, cudaMemcpyAsync(rows, s->contacts, (size_t)n * sizeof(kdop_contact), cudaMemcpyDeviceToHost,
+  KDOP_CUDA(s->ctx, cudaMemcpyAsync(rows, s->contacts, (size_t)n * sizeof(kdop_contact), cudaMemcpyDefault,
                                     s->ctx->stream));
   KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
   return KDOP_OK;

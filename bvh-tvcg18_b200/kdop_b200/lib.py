@@ -370,6 +370,15 @@ class DeviceScene:
         self.ctx._check(self.lib.kdop_read_contacts(self.h, _ptr(rows), n, C.byref(nr)))
         return rows[:nr.value]
 
+    def read_contacts_into(self, buf) -> int:
+        """Contact rows into `buf` (host array or CUDA tensor of at least
+        32 bytes per row); returns the number of rows."""
+        st = self.stats(check=False)
+        n = min(st.n_contacts, st.contact_capacity)
+        nr = C.c_int64()
+        self.ctx._check(self.lib.kdop_read_contacts(self.h, _ptr(buf), n, C.byref(nr)))
+        return nr.value
+
     def adjoint(self, d_depth, d_normal, grad):
         """grad += dL/d(world vertex positions); arrays host numpy or CUDA tensors."""
         self.ctx._check(self.lib.kdop_contacts_adjoint(self.h, _ptr(d_depth), _ptr(d_normal), _ptr(grad),

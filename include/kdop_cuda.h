@@ -268,7 +268,8 @@ typedef struct {
  * of the last traversal.  Asynchronous. */
 int kdop_contacts(kdop_scene* scene);
 /* Contacts grouped by candidate (rows of one candidate are contiguous, in the
- * reference's reporting order).  Synchronises. */
+ * reference's reporting order).  `rows` may be host or device memory (a
+ * device buffer gets a device-to-device copy).  Synchronises. */
 int kdop_read_contacts(kdop_scene* scene, kdop_contact* rows, int64_t cap_rows, int64_t* n_rows);
 
 /* Puts the last traversal's results in a reproducible order, on the device:
