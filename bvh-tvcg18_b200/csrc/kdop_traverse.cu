@@ -404,20 +404,22 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         if (valid) {
           if (gq == 0) tests32 += (singleA ? 1u : 2u) * (singleB ? 1u : 2u);
 #pragma unroll
+          const uint32_t filt = a.surface_filter ? (LEAF_BIT | SURF_BIT) : LEAF_BIT;
+#pragma unroll
           for (int r = 0; r < PM; ++r) {
             const int c = gq + Q * r;
-            if (c >= 4 || (sep & (1u << c))) continue;
-            const uint32_t wa = (c >> 1) ? wA1 : wA0, wb = (c & 1) ? wB1 : wB0;
+            // child pair c = 2 i + k; with two lanes per entry i = r and k = the lane
+            const int ci = (Q == 2) ? r : (c >> 1), ck = (Q == 2) ? gq : (c & 1);
+            if ((Q * r + Q - 1 >= 4 && c >= 4) || ((sep >> c) & 1u)) continue;
+            const uint32_t wa = ci ? wA1 : wA0, wb = ck ? wB1 : wB0;
             const int k = b * PM + r;
             pushA[k] = wa;
             pushB[k] = wb;
             slotP[k] = ep[b];
-            if (wa & wb & LEAF_BIT) {
-              lo32 += 1u;
-              if (!a.surface_filter || (wa & wb & SURF_BIT)) emit_mask |= 1u << k;
-            } else {
-              push_mask |= 1u << k;
-            }
+            const uint32_t both = wa & wb;
+            lo32 += both >> 31;  // both leaves
+            emit_mask |= ((both & filt) == filt ? 1u : 0u) << k;
+            push_mask |= (both & LEAF_BIT ? 0u : 1u) << k;
           }
         }
       }
