@@ -74,6 +74,12 @@ struct kdop_scene_ext {
   size_t sort_work_bytes = 0;
   void* shard_work = nullptr;  // kdop_traverse_shard scratch
   size_t shard_work_bytes = 0;
+  unsigned* radius_bits = nullptr;  // broad phase: bounding radius per mesh (float bits)
+  void* broad_work = nullptr;
+  size_t broad_work_bytes = 0;
+  uint2* broad_pairs = nullptr;
+  int64_t broad_cap = 0;
+  float* broad_pos = nullptr;
   std::vector<uint32_t> pairs_host;  // last traversed mesh pairs
   std::vector<uint32_t> order_host;  // their order of processing
   int64_t graph_kernels = 0;
@@ -233,6 +239,16 @@ static void scene_free(kdop_scene* s) {
   if (x->shard_work) cudaFree(x->shard_work);
   x->shard_work = nullptr;
   x->shard_work_bytes = 0;
+  if (x->radius_bits) cudaFree(x->radius_bits);
+  if (x->broad_work) cudaFree(x->broad_work);
+  if (x->broad_pairs) cudaFree(x->broad_pairs);
+  if (x->broad_pos) cudaFree(x->broad_pos);
+  x->radius_bits = nullptr;
+  x->broad_work = nullptr;
+  x->broad_pairs = nullptr;
+  x->broad_pos = nullptr;
+  x->broad_work_bytes = 0;
+  x->broad_cap = 0;
 }
 
 // A captured graph holds the buffer addresses of its capture: any
@@ -777,6 +793,56 @@ int kdop_traverse(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   s->last_pairs = n_pairs;
   s->last_mode = mode;
   s->last_params = p;
+  return KDOP_OK;
+}
+
+int kdop_broad_phase(kdop_scene* s, const float* positions, int memory, uint32_t* out_pairs, int64_t cap,
+                     int64_t* n_pairs) {
+  if (!s || !n_pairs || cap < 0 || (cap > 0 && !out_pairs)) return KDOP_ERR_INVALID;
+  if (memory != KDOP_HOST && memory != KDOP_DEVICE) return fail(s->ctx, KDOP_ERR_INVALID, "bad memory kind");
+  cudaSetDevice(s->ctx->device);
+  cudaStream_t st = s->ctx->stream;
+  kdop_scene_ext* x = ext(s);
+  const int n = s->n_meshes;
+  *n_pairs = 0;
+  if (!x->radius_bits) {
+    KDOP_CUDA(s->ctx, cudaMalloc((void**)&x->radius_bits, (size_t)std::max(n, 1) * 4));
+    s->device_bytes += (int64_t)std::max(n, 1) * 4;
+    KDOP_CUDA(s->ctx, kdop::launch_mesh_radius(s, x->radius_bits));
+  }
+  size_t need = kdop::broad_work_bytes(n);
+  if (x->broad_work_bytes < need) {
+    if (x->broad_work) cudaFree(x->broad_work);
+    x->broad_work = nullptr;
+    KDOP_CUDA(s->ctx, cudaMalloc(&x->broad_work, need));
+    s->device_bytes += (int64_t)need - (int64_t)x->broad_work_bytes;
+    x->broad_work_bytes = need;
+  }
+  const float* pos = positions;
+  if (positions && memory == KDOP_HOST) {
+    if (!x->broad_pos) {
+      KDOP_CUDA(s->ctx, cudaMalloc((void**)&x->broad_pos, (size_t)std::max(n, 1) * 12));
+      s->device_bytes += (int64_t)std::max(n, 1) * 12;
+    }
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(x->broad_pos, positions, (size_t)n * 12, cudaMemcpyHostToDevice, st));
+    pos = x->broad_pos;
+  }
+  int64_t total = 0;
+  KDOP_CUDA(s->ctx, kdop::broad_phase(s, x->radius_bits, pos, x->broad_work, x->broad_pairs, x->broad_cap, &total));
+  if (total > x->broad_cap) {
+    if (x->broad_pairs) cudaFree(x->broad_pairs);
+    x->broad_pairs = nullptr;
+    int64_t c = total + total / 4 + 256;
+    KDOP_CUDA(s->ctx, cudaMalloc((void**)&x->broad_pairs, (size_t)c * sizeof(uint2)));
+    s->device_bytes += (c - x->broad_cap) * (int64_t)sizeof(uint2);
+    x->broad_cap = c;
+    KDOP_CUDA(s->ctx, kdop::broad_phase(s, x->radius_bits, pos, x->broad_work, x->broad_pairs, x->broad_cap, &total));
+  }
+  *n_pairs = total;
+  if (total > cap) return fail(s->ctx, KDOP_ERR_CAPACITY, "broad phase: output buffer too small");
+  if (total > 0)
+    KDOP_CUDA(s->ctx, cudaMemcpyAsync(out_pairs, x->broad_pairs, (size_t)total * sizeof(uint2), cudaMemcpyDefault, st));
+  KDOP_CUDA(s->ctx, cudaStreamSynchronize(st));
   return KDOP_OK;
 }
 

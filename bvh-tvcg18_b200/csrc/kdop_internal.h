@@ -200,6 +200,11 @@ void surface_map(int64_t n_tets, const uint32_t* tets, uint8_t* surf);
 cudaError_t launch_write_topology(kdop_scene* s, const uint32_t* topo_dev);
 cudaError_t launch_refit(kdop_scene* s, int mode);
 cudaError_t launch_traverse(kdop_scene* s, int64_t n_pairs, const uint2* pairs, const TravParams& p, int plain);
+// broad phase (kdop_broad.cu)
+cudaError_t launch_mesh_radius(kdop_scene* s, unsigned* rbits);
+size_t broad_work_bytes(int n);
+cudaError_t broad_phase(kdop_scene* s, const unsigned* rbits, const float* pos_dev, void* work, uint2* pairs,
+                        int64_t cap, int64_t* total);
 // Frontier-seeded traversal of shard `rank` of `n_ranks` (synchronises once,
 // for the frontier's size); *work / *work_bytes: the scene's scratch for it,
 // grown here; *n_entries = frontier pairs this shard started from.

@@ -403,7 +403,6 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         const uint32_t wB1 = __shfl_sync(0xffffffffu, t3, src);
         if (valid) {
           if (gq == 0) tests32 += (singleA ? 1u : 2u) * (singleB ? 1u : 2u);
-#pragma unroll
           const uint32_t filt = a.surface_filter ? (LEAF_BIT | SURF_BIT) : LEAF_BIT;
 #pragma unroll
           for (int r = 0; r < PM; ++r) {

@@ -114,6 +114,7 @@ def load_library():
         "kdop_read_candidates": ([vp, vp, i64, C.POINTER(i64)], i32),
         "kdop_contacts": ([vp], i32),
         "kdop_sort_results": ([vp], i32),
+        "kdop_broad_phase": ([vp, vp, i32, vp, i64, C.POINTER(i64)], i32),
         "kdop_traverse_shard": ([vp, i64, vp, i32, C.POINTER(TraverseOpts), i32, i32, i64], i32),
         "kdop_read_contacts": ([vp, vp, i64, C.POINTER(i64)], i32),
         "kdop_contacts_adjoint": ([vp, vp, vp, vp, i32], i32),
@@ -297,6 +298,22 @@ class DeviceScene:
         self.pairs = p
         self.ctx._check(self.lib.kdop_traverse(self.h, n, _ptr(p), _mem(p), C.byref(opts) if opts else None),
                         "kdop_traverse")
+
+    def broad_phase(self, positions=None) -> np.ndarray:
+        """(n, 2) uint32 mesh pairs whose bounding boxes overlap (i < j, sorted);
+        positions: (n_meshes, 3) or None for the poses of set_poses."""
+        pos = None if positions is None else _arg(positions, np.float32)
+        n = C.c_int64()
+        cap = 1 << 16
+        while True:
+            out = np.zeros((cap, 2), np.uint32)
+            rc = self.lib.kdop_broad_phase(self.h, _ptr(pos), _mem(pos) if pos is not None else HOST, _ptr(out), cap,
+                                           C.byref(n))
+            if rc == ERR_CAPACITY and n.value > cap:
+                cap = n.value
+                continue
+            self.ctx._check(rc, "kdop_broad_phase")
+            return out[:n.value]
 
     def traverse_shard(self, pairs, rank: int, n_ranks: int, frontier_min: int = 16384,
                        opts: Optional[TraverseOpts] = None):

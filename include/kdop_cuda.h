@@ -199,6 +199,19 @@ typedef struct {
 /* Enqueues the traversal of n_pairs mesh pairs (pairs[2i] = mesh A, pairs[2i+1]
  * = mesh B).  Asynchronous: read results with kdop_get_stats.  opts NULL =
  * defaults. */
+/* Broad phase (replaces broad::find_overlaps, SIMULATION/BROAD/BROAD/include/
+ * broad_find_overlaps.h:44-125; its all-pair and grid algorithms report the
+ * same set): the mesh pairs (i, j), i < j, whose boxes overlap, sorted
+ * lexicographically -- the pair list kdop_traverse takes.  A mesh's box is
+ * its position +- its bounding radius (prox_rigid_body.h:159-172), the radius
+ * the largest |rest vertex| (narrow_shape_types.h:189-206); boxes overlap
+ * unless one's max is strictly below the other's min on an axis.
+ * positions: n_meshes * 3 floats in `memory`, or NULL for the positions of
+ * kdop_set_poses.  out_pairs: room for `cap` pairs, host or device memory;
+ * *n_pairs = pairs found (KDOP_ERR_CAPACITY when above cap).  Synchronises. */
+int kdop_broad_phase(kdop_scene* scene, const float* positions, int memory, uint32_t* out_pairs, int64_t cap,
+                     int64_t* n_pairs);
+
 int kdop_traverse(kdop_scene* scene, int64_t n_pairs, const uint32_t* pairs, int memory,
                   const kdop_traverse_opts* opts);
 

@@ -246,6 +246,33 @@ class Oracle:
     def sin(self, x: float) -> float:
         return float(self.lib.or_sin_f(C.c_float(x)))
 
+    @staticmethod
+    def mesh_radius(xyz) -> np.float32:
+        """Bounding radius of a mesh: max |r0| over its rest vertices, norm as
+        sqrt(((x*x) + (y*y)) + (z*z)) in float (narrow_shape_types.h:189-206)."""
+        x = _c(xyz, np.float32)
+        if len(x) == 0:
+            return np.float32(0)
+        d = (x[:, 0] * x[:, 0] + x[:, 1] * x[:, 1]) + x[:, 2] * x[:, 2]
+        return np.float32(np.sqrt(d.astype(np.float32)).max())
+
+    @staticmethod
+    def broad_pairs(pos, radius) -> np.ndarray:
+        """All-pair broad phase (broad_find_overlaps.h:44-125): boxes
+        pos +- radius (prox_rigid_body.h:159-172) in float; (i, j), i < j,
+        overlapping unless a max is strictly below a min; sorted."""
+        p = _c(pos, np.float32)
+        r = _c(radius, np.float32)
+        lo = p - r[:, None]
+        hi = p + r[:, None]
+        n = len(p)
+        out = []
+        for i in range(n - 1):
+            sep = (hi[i + 1:] < lo[i]) | (hi[i] < lo[i + 1:])
+            js = np.nonzero(~sep.any(axis=1))[0] + i + 1
+            out += [(i, int(j)) for j in js]
+        return np.array(out, np.uint32).reshape(-1, 2)
+
     def deform(self, amp, w, phase, xyz) -> np.ndarray:
         xyz = _c(xyz, np.float32)
         out = np.zeros_like(xyz)
@@ -264,6 +291,10 @@ class Reference:
         L.ref_rotate.argtypes = [_p, _p, C.c_int, _p, _p]
         L.ref_direction_table.argtypes = [C.c_int, _p]
         L.ref_contacts_pairs.argtypes = [C.c_int, _p, _p, _p, _p, _p, _p, C.c_longlong, _p, C.c_longlong, _p, _p]
+        if hasattr(L, "ref_broad_pairs"):
+            L.ref_broad_pairs.argtypes = [C.c_int, _p, _p, C.c_int, _p, C.c_longlong, _p]
+            L.ref_mesh_radius.argtypes = [C.c_int, _p]
+            L.ref_mesh_radius.restype = C.c_float
         if hasattr(L, "ref_traverse"):
             L.ref_traverse.argtypes = [C.c_int, C.c_ulonglong, C.c_int, C.c_int, _p, _p, _p, C.c_int, _p,
                                        C.c_int, _p, _p, _p, C.c_int, _p, C.c_longlong, _p, _p, C.c_longlong, _p,
@@ -274,6 +305,22 @@ class Reference:
         out = np.zeros(tets.shape[0], np.uint8)
         self.lib.ref_surface_map(xyz.shape[0], _ptr(xyz), tets.shape[0], _ptr(tets), _ptr(out))
         return out
+
+    def broad_pairs(self, pos, radius, algorithm: int = 0) -> np.ndarray:
+        """broad::find_overlaps over boxes pos +- radius: 0 all-pair, 1 grid."""
+        pos, radius = _c(pos, np.float32), _c(radius, np.float32)
+        n = len(pos)
+        cap = max(n * (n - 1) // 2, 1)
+        out = np.zeros((cap, 2), np.uint32)
+        cnt = C.c_longlong()
+        rc = self.lib.ref_broad_pairs(n, _ptr(pos), _ptr(radius), algorithm, _ptr(out), cap, C.byref(cnt))
+        if rc != 0:
+            raise RuntimeError(f"ref_broad_pairs failed: {rc}")
+        return out[:cnt.value]
+
+    def mesh_radius(self, xyz) -> np.float32:
+        xyz = _c(xyz, np.float32)
+        return np.float32(self.lib.ref_mesh_radius(len(xyz), _ptr(xyz)))
 
     def mesh_reorder(self, xyz, tets):
         xyz, tets = _c(xyz, np.float32), _c(tets, np.uint32)

@@ -97,6 +97,7 @@ class SelectContactPointAlgorithm {
 #include <kdop_mesh_reorder.h>
 #include <kdop_test_pair.h>
 #include <kdop_tandem_traversal.h>
+#include <broad.h>
 
 namespace refh {
 #if REF_RECORD
@@ -601,6 +602,65 @@ int ref_time_pairs(int K, unsigned long long mem_bytes, int n_meshes, long long 
   }
 #undef REFH_TP
   return -1;
+}
+
+
+// Broad phase of the reference (broad_find_overlaps.h): every body a box of
+// its position +- its bounding radius (prox_rigid_body.h:159-172); overlapping
+// body pairs (lower index first, lexicographically sorted) by the all-pair
+// (algorithm 0) or the grid (1) algorithm.
+struct RefBox : public broad::Object<float> {
+  float x, y, z, r;
+  void get_box(float& mx, float& my, float& mz, float& Mx, float& My, float& Mz) const {
+    mx = x - r;
+    my = y - r;
+    mz = z - r;
+    Mx = x + r;
+    My = y + r;
+    Mz = z + r;
+  }
+};
+
+int ref_broad_pairs(int n, float const* pos, float const* radius, int algorithm, unsigned* out, long long cap,
+                    long long* n_out) {
+  util::LogInfo::console() = false;
+  util::LogInfo::on() = false;
+  std::vector<RefBox> boxes((size_t)n);
+  broad::System<float> sys;
+  for (int i = 0; i < n; ++i) {
+    boxes[i].x = pos[3 * i];
+    boxes[i].y = pos[3 * i + 1];
+    boxes[i].z = pos[3 * i + 2];
+    boxes[i].r = radius[i];
+    sys.connect(&boxes[i]);
+  }
+  std::vector<std::pair<broad::Object<float>*, broad::Object<float>*> > overlaps;
+  float eff = 0.f;
+  if (algorithm == 1) {
+    sys.compute_optimal_cell_spacing();
+    broad::find_overlaps(sys, overlaps, eff, broad::grid_algorithm());
+  } else {
+    broad::find_overlaps(sys, overlaps, eff, broad::all_pair_algorithm());
+  }
+  *n_out = (long long)overlaps.size();
+  if ((long long)overlaps.size() > cap) return -2;
+  for (size_t k = 0; k < overlaps.size(); ++k) {
+    out[2 * k] = (unsigned)(static_cast<RefBox*>(overlaps[k].first) - boxes.data());
+    out[2 * k + 1] = (unsigned)(static_cast<RefBox*>(overlaps[k].second) - boxes.data());
+  }
+  return 0;
+}
+
+// Bounding radius of a mesh about its body origin: max |r0| over the rest
+// vertices (narrow_shape_types.h:189-206).
+float ref_mesh_radius(int nv, float const* xyz) {
+  typedef tiny::MathTypes<float>::vector3_type V;
+  float r = 0.f;
+  for (int i = 0; i < nv; ++i) {
+    V const r0 = V::make(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    r = std::max(r, tiny::norm(r0));
+  }
+  return r;
 }
 
 }  // extern "C"

@@ -94,6 +94,19 @@ def main():
         g[f"{key}_tests"] = np.int64(r["tests"])
         g[f"{key}_contacts_f32"] = r["contacts"]
         g[f"{key}_contacts_f64"] = R.contacts(xa, A.tets, A.surf, xb, B.tets, B.surf, r["pairs"], fp64=True)
+    # broad phase: 300 bodies, positions on a coarse grid so that some boxes
+    # touch exactly (equal max and min count as overlapping), radii of the
+    # meshes of a small batch
+    rng = np.random.default_rng(77)
+    pos = (rng.integers(0, 24, size=(300, 3)) * 0.5).astype(np.float32)
+    rad = np.float32(0.25) * rng.integers(1, 5, size=300).astype(np.float32)
+    g["broad_pos"], g["broad_radius"] = pos, rad
+    g["broad_pairs"] = R.broad_pairs(pos, rad, 0)
+    g["broad_pairs_grid"] = R.broad_pairs(pos, rad, 1)
+    sb = scenes.small_batch(n_pairs=4, seed=9)
+    g["radius_xyz"] = np.concatenate([m.xyz for m in sb.meshes])
+    g["radius_n"] = np.array([m.n_verts for m in sb.meshes], np.int64)
+    g["radius_out"] = np.array([R.mesh_radius(m.xyz) for m in sb.meshes], np.float32)
     np.savez_compressed(os.path.join(OUT, "reference_golden.npz"), **g)
     print("wrote", os.path.join(OUT, "reference_golden.npz"), os.path.getsize(os.path.join(OUT, "reference_golden.npz")),
           "bytes")

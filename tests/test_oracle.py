@@ -106,3 +106,25 @@ def test_oracle_against_reference_random(oracle, reference, K, seed):
     assert tests == r["tests"]
     cf, _ = oracle.contacts(a.xyz, a.tets, a.surf, xb, b.tets, b.surf, pairs, "f")
     assert cf.tobytes() == r["contacts"].tobytes()
+
+
+def test_broad_phase_oracle_against_golden(oracle, golden):
+    pos, rad = golden["broad_pos"], golden["broad_radius"]
+    got = oracle.broad_pairs(pos, rad)
+    assert np.array_equal(got, golden["broad_pairs"])
+    # the reference's grid algorithm reports the same sorted set
+    assert np.array_equal(golden["broad_pairs_grid"], golden["broad_pairs"])
+    xyz, n = golden["radius_xyz"], golden["radius_n"]
+    off = np.concatenate([[0], np.cumsum(n)])
+    r = np.array([oracle.mesh_radius(xyz[off[i]:off[i + 1]]) for i in range(len(n))], np.float32)
+    assert np.array_equal(r.view(np.uint32), golden["radius_out"].view(np.uint32))
+
+
+def test_broad_phase_oracle_against_reference_random(oracle, reference):
+    rng = np.random.default_rng(5)
+    for n in (1, 2, 17, 150):
+        pos = (rng.random((n, 3)) * 10).astype(np.float32)
+        rad = (rng.random(n) * 1.5 + 0.05).astype(np.float32)
+        want = reference.broad_pairs(pos, rad, 0)
+        assert np.array_equal(oracle.broad_pairs(pos, rad), want)
+        assert np.array_equal(reference.broad_pairs(pos, rad, 1), want)
