@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--pairs", type=int, default=0, help="mesh pairs per GPU (config3: 512, config5: 256)")
-    ap.add_argument("--workload", default="config3", choices=["config3", "config2", "config5", "config1"],
+    ap.add_argument("--workload", default="config3", choices=["config3", "config2", "config4", "config5", "config1"],
                     help="config3 is the headline; the others are the same step on the other configs")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -190,6 +190,8 @@ def workload(args, rank: int):
         return scenes.config2()
     if args.workload == "config5":
         return scenes.config5(n_pairs=args.pairs or 256)
+    if args.workload == "config4":
+        return scenes.config4(n_pairs=args.pairs or 64)
     if args.workload == "config1":
         return scenes.config1()
     return scenes.config3(n_pairs=args.pairs or 512, seed=2 + rank)
@@ -381,7 +383,14 @@ def run_cuda(args):
     ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
     info = ds.info()
     ds.set_poses(sc.quat, sc.pos)
-    ds.refit(kd.REFIT_POSE)
+    # config 4 deforms and moves every step (motion integrated inside the graph)
+    deforming = args.workload == "config4"
+    refit_mode = kd.REFIT_DEFORM if deforming else kd.REFIT_POSE
+    if deforming:
+        ex = sc.extra
+        ds.set_deformation(ex["amp"], float(np.float32(2 * np.pi / ex["L"])), 0.0)
+        ds.set_motion(ex["lin_vel"], ex["ang_vel"], ex["phase_rate"])
+    ds.refit(refit_mode)
     st = ds.traverse_sync(sc.pairs, contacts=True)
     tuned = None
     if args.opts:
@@ -395,8 +404,9 @@ def run_cuda(args):
     ds.reserve(candidates=int(st.n_candidates * 1.2) + 1024, contacts=int(st.n_contacts * 1.2) + 1024,
                queue=max(st.queue_used * 2, 1 << 20))
 
-    # one step = motion-free pose refit + traversal + contacts in one CUDA graph
-    ds.graph_capture(sc.pairs, refit_mode=kd.REFIT_POSE, opts=opts)
+    # one step = pose refit + traversal + contacts in one CUDA graph (config 4:
+    # motion update + deforming refit + traversal + contacts)
+    ds.graph_capture(sc.pairs, refit_mode=refit_mode, opts=opts, motion=deforming)
     launches0 = ctx.launches
     for _ in range(args.warmup):
         ds.graph_launch()
@@ -409,17 +419,32 @@ def run_cuda(args):
     e1 = torch.cuda.Event(enable_timing=True)
     ctx.synchronize()
     launches_before = ctx.launches
-    e0.record(stream)
-    for _ in range(args.steps):
-        ds.graph_launch()
-    e1.record(stream)
-    e1.synchronize()
+    if deforming:
+        # the state moves every step: time each step, count its own tests
+        total_ms, total_tests = 0.0, 0
+        for _ in range(args.steps):
+            e0.record(stream)
+            ds.graph_launch()
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            total_tests += ds.stats().n_tests
+        ms = total_ms / args.steps
+        tests_per_step = total_tests / args.steps
+    else:
+        e0.record(stream)
+        for _ in range(args.steps):
+            ds.graph_launch()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
     launches_timed = ctx.launches - launches_before
-    ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
     dist.barrier()
     st2 = ds.stats()
-    assert st2.n_tests == tests_per_step, (st2.n_tests, tests_per_step)
+    state_tests = st2.n_tests  # tests of the state the later timings traverse
+    if not deforming:  # a fixed state makes the same tests every step
+        assert state_tests == tests_per_step, (state_tests, tests_per_step)
     ms_max = dist.max(ms)
     total_tests = dist.sum(float(tests_per_step))
     value = total_tests / (ms_max * 1e-3)
@@ -437,7 +462,7 @@ def run_cuda(args):
         tt.append(a0.elapsed_time(a1))
     trav_ms = statistics.median(tt[1:])
     node_bytes = info["node_bytes"]
-    alg_bytes = tests_per_step * 2 * node_bytes
+    alg_bytes = state_tests * 2 * node_bytes
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (trav_ms * 1e-3) / 1e9
     traffic = ncu_traffic("traverse_config3.md") if args.workload == "config3" else None
@@ -465,11 +490,11 @@ def run_cuda(args):
                 a1.synchronize()
                 pt.append(a0.elapsed_time(a1))
             pst = ds.stats()
-            assert pst.n_tests == tests_per_step
+            assert pst.n_tests == state_tests
             if best is None or min(pt) < best[0]:
                 best = (min(pt), name, popts.as_dict())
         plain_ms = best[0]
-        plain = {"traversal_ms": plain_ms, "tests_per_s": tests_per_step / (plain_ms * 1e-3),
+        plain = {"traversal_ms": plain_ms, "tests_per_s": state_tests / (plain_ms * 1e-3),
                  "batched_speedup": plain_ms / trav_ms, "launch_shape": best[1], "opts": best[2]}
 
     # e2e: through the public API with host buffers; per step the world
@@ -511,9 +536,12 @@ def run_cuda(args):
     b1.record(stream)
     b1.synchronize()
     e2e_ms = max(b0.elapsed_time(b1), (time.perf_counter() - w0) * 1e3) / args.e2e_steps
-    assert s.n_tests == tests_per_step
+    if not deforming:
+        assert s.n_tests == tests_per_step
     e2e_ms_max = dist.max(e2e_ms)
-    e2e_value = total_tests / (e2e_ms_max * 1e-3)
+    # the end-to-end step traverses the rigidly posed meshes (config 4: without
+    # its deformation), so it is rated by its own test count
+    e2e_value = dist.sum(float(s.n_tests)) / (e2e_ms_max * 1e-3)
     h2d = world.nbytes + sc.pairs.nbytes
     d2h = ncont * 32 + 128
 
