@@ -347,11 +347,11 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
 #pragma unroll
         for (int r = 0; r < C; ++r) {
           const int j = gq + Q * r;
-          if (i < n && j < NW) {
+          // a lane without an entry (i >= n) loads the record of node 0's
+          // twin and its verdicts are never used: no zero fill
+          if (j < NW) {
             ldg256(a.nodes + ta + 2 * j, A0[b][r], A1[b][r]);
             ldg256(a.nodes + tb + 2 * j, B0[b][r], B1[b][r]);
-          } else {
-            A0[b][r] = A1[b][r] = B0[b][r] = B1[b][r] = make_float4(0.f, 0.f, 0.f, 0.f);
           }
         }
       }
@@ -403,23 +403,29 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         const uint32_t wB1 = __shfl_sync(0xffffffffu, t3, src);
         if (valid) {
           if (gq == 0) tests32 += (singleA ? 1u : 2u) * (singleB ? 1u : 2u);
-          const uint32_t filt = a.surface_filter ? (LEAF_BIT | SURF_BIT) : LEAF_BIT;
+          // the lane's child pairs c = gq + Q r (c = 2 i + k: child i of A,
+          // child k of B) as bit masks: overlapping, both leaves, both on
+          // the surface
+          unsigned alive = 0, leaf = 0, surf = 0;
 #pragma unroll
           for (int r = 0; r < PM; ++r) {
             const int c = gq + Q * r;
-            // child pair c = 2 i + k; with two lanes per entry i = r and k = the lane
             const int ci = (Q == 2) ? r : (c >> 1), ck = (Q == 2) ? gq : (c & 1);
-            if ((Q * r + Q - 1 >= 4 && c >= 4) || ((sep >> c) & 1u)) continue;
             const uint32_t wa = ci ? wA1 : wA0, wb = ck ? wB1 : wB0;
+            const uint32_t both = wa & wb;
             const int k = b * PM + r;
             pushA[k] = wa;
             pushB[k] = wb;
             slotP[k] = ep[b];
-            const uint32_t both = wa & wb;
-            lo32 += both >> 31;  // both leaves
-            emit_mask |= ((both & filt) == filt ? 1u : 0u) << k;
-            push_mask |= (both & LEAF_BIT ? 0u : 1u) << k;
+            const bool ok = (Q * r + Q - 1 < 4 || c < 4) && !((sep >> c) & 1u);
+            alive |= (ok ? 1u : 0u) << r;
+            leaf |= (both >> 31) << r;
+            surf |= ((both >> 30) & 1u) << r;
           }
+          if (!a.surface_filter) surf = ~0u;
+          lo32 += __popc(alive & leaf);  // both leaves
+          emit_mask |= (alive & leaf & surf) << (b * PM);
+          push_mask |= (alive & ~leaf & ((1u << PM) - 1u)) << (b * PM);
         }
       }
     }
@@ -491,7 +497,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
       }
     }
     int depth = top - bot;
-    if ((unsigned)depth > max_depth) max_depth = (unsigned)depth;
+    if (polled && (unsigned)depth > max_depth) max_depth = (unsigned)depth;
 
     // ---- donation: give the oldest entries to waiting warps ----
     // A deep deque gives to any waiting warp; while many warps wait (the
