@@ -1023,6 +1023,76 @@ int kdop_read_contacts(kdop_scene* s, kdop_contact* rows, int64_t cap, int64_t* 
   return KDOP_OK;
 }
 
+// ---- contact reduction (prox_collision_detection.h:341-350) ----
+// Reduces n device rows with their device bodies into scratch, then copies
+// the kept rows (and bodies) to the caller's buffers (host or device).
+static int reduce_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint2* bodies, int64_t n, kdop_contact* out,
+                       uint32_t* out_bodies, int64_t cap, int64_t* n_out) {
+  const size_t wb = (kdop::reduce_work_bytes(n) + 255) & ~(size_t)255;
+  const size_t rb = ((size_t)std::max<int64_t>(n, 1) * sizeof(kdop_contact) + 255) & ~(size_t)255;
+  char* buf = nullptr;
+  KDOP_CUDA(ctx, cudaMalloc((void**)&buf, wb + rb + (size_t)std::max<int64_t>(n, 1) * sizeof(uint2)));
+  kdop_contact* kept_rows = reinterpret_cast<kdop_contact*>(buf + wb);
+  uint2* kept_bodies = reinterpret_cast<uint2*>(buf + wb + rb);
+  int64_t kept = 0;
+  cudaError_t e = kdop::reduce_contact_rows(ctx, rows, bodies, n, buf, kept_rows, kept_bodies, &kept);
+  int rc = KDOP_OK;
+  *n_out = kept;
+  if (e != cudaSuccess) {
+    rc = cuda_fail(ctx, e, "reduce_contact_rows");
+  } else if (kept > cap) {
+    rc = fail(ctx, KDOP_ERR_CAPACITY, "reduced contact buffer too small");
+  } else if (kept > 0) {
+    e = cudaMemcpyAsync(out, kept_rows, (size_t)kept * sizeof(kdop_contact), cudaMemcpyDefault, ctx->stream);
+    if (e == cudaSuccess && out_bodies)
+      e = cudaMemcpyAsync(out_bodies, kept_bodies, (size_t)kept * sizeof(uint2), cudaMemcpyDefault, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "reduced contacts copy");
+  }
+  cudaFree(buf);
+  return rc;
+}
+
+int kdop_reduce_contact_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint32_t* bodies, int64_t n,
+                             kdop_contact* out, uint32_t* out_bodies, int64_t cap, int64_t* n_out) {
+  if (!ctx || !n_out || n < 0 || (n > 0 && (!rows || !bodies)) || (cap > 0 && !out)) return KDOP_ERR_INVALID;
+  if (n >= ((int64_t)1 << 32) - 1) return fail(ctx, KDOP_ERR_INVALID, "too many contact rows");
+  *n_out = 0;
+  if (n == 0) return KDOP_OK;
+  cudaSetDevice(ctx->device);
+  const size_t rb = ((size_t)n * sizeof(kdop_contact) + 255) & ~(size_t)255;
+  char* in = nullptr;
+  KDOP_CUDA(ctx, cudaMalloc((void**)&in, rb + (size_t)n * sizeof(uint2)));
+  cudaError_t e = cudaMemcpyAsync(in, rows, (size_t)n * sizeof(kdop_contact), cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(in + rb, bodies, (size_t)n * sizeof(uint2), cudaMemcpyDefault, ctx->stream);
+  int rc = e != cudaSuccess ? cuda_fail(ctx, e, "reduce input copy")
+                            : reduce_rows(ctx, reinterpret_cast<kdop_contact*>(in), reinterpret_cast<uint2*>(in + rb),
+                                          n, out, out_bodies, cap, n_out);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(in);
+  return rc;
+}
+
+int kdop_reduce_contacts(kdop_scene* s, kdop_contact* out, uint32_t* out_bodies, int64_t cap, int64_t* n_out) {
+  if (!s || !n_out || (cap > 0 && !out)) return KDOP_ERR_INVALID;
+  if (!s->contacted) return fail(s->ctx, KDOP_ERR_STATE, "kdop_reduce_contacts before kdop_contacts");
+  kdop_stats st;
+  int rc = kdop_get_stats(s, &st);  // synchronises; reports overflow and device errors
+  if (rc != KDOP_OK) return rc;
+  const int64_t n = std::min<int64_t>(st.n_contacts, s->contact_cap);
+  *n_out = 0;
+  if (n <= 0) return KDOP_OK;
+  uint2* bodies = nullptr;
+  KDOP_CUDA(s->ctx, cudaMalloc((void**)&bodies, (size_t)n * sizeof(uint2)));
+  cudaError_t e = kdop::scene_contact_bodies(s, n, bodies);
+  rc = e != cudaSuccess ? cuda_fail(s->ctx, e, "scene_contact_bodies")
+                        : reduce_rows(s->ctx, s->contacts, bodies, n, out, out_bodies, cap, n_out);
+  cudaStreamSynchronize(s->ctx->stream);
+  cudaFree(bodies);
+  return rc;
+}
+
 int kdop_contacts_adjoint(kdop_scene* s, const float* dd, const float* dn, float* grad, int memory) {
   if (!s || !dd || !grad) return KDOP_ERR_INVALID;
   if (!s->contacted) return fail(s->ctx, KDOP_ERR_STATE, "adjoint before kdop_contacts");

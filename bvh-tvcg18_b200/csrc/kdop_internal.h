@@ -212,6 +212,11 @@ cudaError_t launch_traverse_shard(kdop_scene* s, int64_t n_pairs, const uint2* p
                                   int n_ranks, int64_t frontier_min, void** work, size_t* work_bytes,
                                   int64_t* n_entries);
 cudaError_t launch_contacts(kdop_scene* s);
+// contact reduction (kdop_reduce.cu)
+size_t reduce_work_bytes(int64_t n);
+cudaError_t reduce_contact_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint2* bodies, int64_t n, void* work,
+                                kdop_contact* out, uint2* out_bodies, int64_t* n_out);
+cudaError_t scene_contact_bodies(kdop_scene* s, int64_t n, uint2* bodies);
 cudaError_t launch_adjoint(kdop_scene* s, const float* dd, const float* dn, float* grad);
 cudaError_t launch_motion(kdop_scene* s);
 cudaError_t launch_world(kdop_scene* s, int mode, float4* out);

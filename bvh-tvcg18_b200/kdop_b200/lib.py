@@ -117,6 +117,8 @@ def load_library():
         "kdop_broad_phase": ([vp, vp, i32, vp, i64, C.POINTER(i64)], i32),
         "kdop_traverse_shard": ([vp, i64, vp, i32, C.POINTER(TraverseOpts), i32, i32, i64], i32),
         "kdop_read_contacts": ([vp, vp, i64, C.POINTER(i64)], i32),
+        "kdop_reduce_contacts": ([vp, vp, vp, i64, C.POINTER(i64)], i32),
+        "kdop_reduce_contact_rows": ([vp, vp, vp, i64, vp, vp, i64, C.POINTER(i64)], i32),
         "kdop_contacts_adjoint": ([vp, vp, vp, vp, i32], i32),
         "kdop_set_motion": ([vp, vp, vp, C.c_float, i32], i32),
         "kdop_graph_capture": ([vp, i32, i64, vp, i32, C.POINTER(TraverseOpts), i32], i32),
@@ -184,6 +186,19 @@ class Context:
             msg = self.lib.kdop_last_error(self.h)
             raise KdopError(rc, (msg.decode() if msg else "") or what)
         return rc
+
+    def reduce_contact_rows(self, rows, bodies):
+        """PROX contact reduction of any rows (CONTACT_DTYPE) with their bodies
+        ((n, 2) uint32) via kdop_reduce_contact_rows: (kept rows, bodies)."""
+        rows = np.ascontiguousarray(rows, CONTACT_DTYPE)
+        bodies = np.ascontiguousarray(bodies, np.uint32).reshape(-1, 2)
+        n = len(rows)
+        out = np.zeros(max(n, 1), CONTACT_DTYPE)
+        ob = np.zeros((max(n, 1), 2), np.uint32)
+        nr = C.c_int64()
+        self._check(self.lib.kdop_reduce_contact_rows(self.h, _ptr(rows), _ptr(bodies), n, _ptr(out), _ptr(ob), n,
+                                                      C.byref(nr)), "kdop_reduce_contact_rows")
+        return out[:nr.value], ob[:nr.value]
 
     @property
     def stream(self) -> int:
@@ -386,6 +401,18 @@ class DeviceScene:
         nr = C.c_int64()
         self.ctx._check(self.lib.kdop_read_contacts(self.h, _ptr(rows), n, C.byref(nr)))
         return rows[:nr.value]
+
+    def reduce_contacts(self):
+        """PROX contact reduction of the last kdop_contacts (kdop_reduce_contacts):
+        (kept rows, their bodies (n, 2) = the meshes of the rows' pairs)."""
+        st = self.stats(check=False)
+        n = min(st.n_contacts, st.contact_capacity)
+        rows = np.zeros(max(n, 1), CONTACT_DTYPE)
+        bodies = np.zeros((max(n, 1), 2), np.uint32)
+        nr = C.c_int64()
+        self.ctx._check(self.lib.kdop_reduce_contacts(self.h, _ptr(rows), _ptr(bodies), n, C.byref(nr)),
+                        "kdop_reduce_contacts")
+        return rows[:nr.value], bodies[:nr.value]
 
     def read_contacts_into(self, buf) -> int:
         """Contact rows into `buf` (host array or CUDA tensor of at least

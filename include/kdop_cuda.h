@@ -285,6 +285,27 @@ int kdop_contacts(kdop_scene* scene);
  * device buffer gets a device-to-device copy).  Synchronises. */
 int kdop_read_contacts(kdop_scene* scene, kdop_contact* rows, int64_t cap_rows, int64_t* n_rows);
 
+/* Contact point reduction of PROX (prox_collision_detection.h:341-350):
+ * the contact rows sorted by ContactPoint::operator< (prox_contact_point.h:
+ * 135-194: body i, body j, p.y, p.x, p.z, n.y, n.x, n.z, depth, each by
+ * float `<`), then std::unique with ContactPoint::operator== (:91-133: same
+ * bodies and every component within working_precision<float>() =
+ * 10 FLT_EPSILON, tiny_precision.h:21-24), which keeps a row only when it
+ * differs from the last row kept.  The kept rows go to `out` (and their
+ * bodies, 2 uint32 per row, to `out_bodies` unless NULL) in that order; host
+ * or device memory.  *n_out = rows kept; KDOP_ERR_CAPACITY (nothing written)
+ * when that exceeds cap.  Rows whose nine key fields all compare equal keep
+ * their input order (std::sort leaves it unspecified; such rows can differ
+ * only in the sign of a zero and in `cand`, and all but the first are
+ * dropped).  Synchronises.
+ *
+ * kdop_reduce_contacts: the scene's contacts of the last kdop_contacts, the
+ * bodies of a row being the meshes (A, B) of its candidate's pair.
+ * kdop_reduce_contact_rows: any n rows (host or device) with their bodies. */
+int kdop_reduce_contacts(kdop_scene* scene, kdop_contact* out, uint32_t* out_bodies, int64_t cap, int64_t* n_out);
+int kdop_reduce_contact_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint32_t* bodies, int64_t n,
+                             kdop_contact* out, uint32_t* out_bodies, int64_t cap, int64_t* n_out);
+
 /* Puts the last traversal's results in a reproducible order, on the device:
  * candidate rows by (pair, tet of A, tet of B) and, after kdop_contacts, the
  * contact rows grouped by candidate in that order (each candidate's rows in

@@ -273,6 +273,47 @@ class Oracle:
             out += [(i, int(j)) for j in js]
         return np.array(out, np.uint32).reshape(-1, 2)
 
+    @staticmethod
+    def reduce_contacts(rows, bodies):
+        """PROX contact point reduction (prox_collision_detection.h:341-350):
+        sort by ContactPoint::operator< (prox_contact_point.h:135-194: body i,
+        body j, p.y, p.x, p.z, n.y, n.x, n.z, depth, each by float `<`), then
+        std::unique with ContactPoint::operator== (:91-133: same bodies and
+        every component |new - kept| not above working_precision<float>() =
+        10 FLT_EPSILON, tiny_precision.h:21-24), which drops a row equal to the
+        last row kept.  rows: (n, 7) float32 (p, n, depth); bodies: (n, 2).
+        Returns (rows, bodies, source index) of the kept rows in sorted order
+        (stable among rows whose keys all compare equal)."""
+        r = _c(rows, np.float32).reshape(-1, 7)
+        b = _c(bodies, np.uint32).reshape(-1, 2)
+        n = len(r)
+        if n == 0:
+            return r.copy(), b.copy(), np.zeros(0, np.int64)
+        # lexsort: last key most significant; float keys compare by value (-0 == +0)
+        order = np.lexsort((r[:, 6], r[:, 5], r[:, 3], r[:, 4], r[:, 2], r[:, 0], r[:, 1], b[:, 1], b[:, 0]))
+        rs, bs = r[order], b[order]
+        eps = np.float32(np.float32(np.finfo(np.float32).eps) * np.float32(10))
+        keep = np.ones(n, bool)
+        # a row whose p.y differs from its predecessor's by more than eps (or
+        # whose bodies differ) cannot equal any earlier row: segments between
+        # such rows are independent; walk each longer one sequentially
+        dy = np.abs(rs[1:, 1] - rs[:-1, 1])
+        brk = np.ones(n, bool)
+        brk[1:] = (dy > eps) | (bs[1:, 0] != bs[:-1, 0]) | (bs[1:, 1] != bs[:-1, 1])
+        starts = np.nonzero(brk)[0]
+        ends = np.append(starts[1:], n)
+        for s0, e0 in zip(starts, ends):
+            if e0 - s0 < 2:
+                continue
+            last = s0
+            for j in range(s0 + 1, e0):
+                d = np.abs(rs[j] - rs[last])
+                if (d > eps).any():  # a NaN difference is not "above" eps
+                    last = j
+                else:
+                    keep[j] = False
+        return rs[keep], bs[keep], order[keep]
+
     def deform(self, amp, w, phase, xyz) -> np.ndarray:
         xyz = _c(xyz, np.float32)
         out = np.zeros_like(xyz)
@@ -295,6 +336,8 @@ class Reference:
             L.ref_broad_pairs.argtypes = [C.c_int, _p, _p, C.c_int, _p, C.c_longlong, _p]
             L.ref_mesh_radius.argtypes = [C.c_int, _p]
             L.ref_mesh_radius.restype = C.c_float
+        if hasattr(L, "ref_reduce_contacts"):
+            L.ref_reduce_contacts.argtypes = [C.c_longlong, _p, _p, C.c_int, _p, _p, _p]
         if hasattr(L, "ref_traverse"):
             L.ref_traverse.argtypes = [C.c_int, C.c_ulonglong, C.c_int, C.c_int, _p, _p, _p, C.c_int, _p,
                                        C.c_int, _p, _p, _p, C.c_int, _p, C.c_longlong, _p, _p, C.c_longlong, _p,
@@ -321,6 +364,21 @@ class Reference:
     def mesh_radius(self, xyz) -> np.float32:
         xyz = _c(xyz, np.float32)
         return np.float32(self.lib.ref_mesh_radius(len(xyz), _ptr(xyz)))
+
+    def reduce_contacts(self, rows, bodies):
+        """PROX's std::sort + std::unique over ContactPoints (the reference's
+        own comparisons); returns the kept (rows, bodies) in order."""
+        r = _c(rows, np.float32).reshape(-1, 7)
+        b = _c(bodies, np.uint32).reshape(-1, 2)
+        n = len(r)
+        out_r = np.zeros((max(n, 1), 7), np.float32)
+        out_b = np.zeros((max(n, 1), 2), np.uint32)
+        cnt = C.c_longlong()
+        nb = int(b.max()) + 1 if n else 1
+        rc = self.lib.ref_reduce_contacts(n, _ptr(r), _ptr(b), nb, _ptr(out_r), _ptr(out_b), C.byref(cnt))
+        if rc != 0:
+            raise RuntimeError(f"ref_reduce_contacts failed: {rc}")
+        return out_r[:cnt.value], out_b[:cnt.value]
 
     def mesh_reorder(self, xyz, tets):
         xyz, tets = _c(xyz, np.float32), _c(tets, np.uint32)

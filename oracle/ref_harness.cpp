@@ -98,6 +98,8 @@ class SelectContactPointAlgorithm {
 #include <kdop_test_pair.h>
 #include <kdop_tandem_traversal.h>
 #include <broad.h>
+#include <prox_math_policy.h>
+#include <prox_contact_point.h>
 
 namespace refh {
 #if REF_RECORD
@@ -661,6 +663,40 @@ float ref_mesh_radius(int nv, float const* xyz) {
     r = std::max(r, tiny::norm(r0));
   }
   return r;
+}
+
+// PROX's contact point reduction (prox_collision_detection.h:341-350) on
+// rows of (p, n, depth) with the bodies (a, b) of each row, through the
+// reference's own ContactPoint comparisons (prox_contact_point.h:91-194),
+// std::sort and std::unique.  out_rows: 7 floats and out_bodies: 2 ids per
+// kept row, in the reduced order.
+int ref_reduce_contacts(long long n, float const* rows, unsigned const* bodies, int n_bodies, float* out_rows,
+                        unsigned* out_bodies, long long* n_out) {
+  typedef prox::MathPolicy<float> M;
+  typedef M::vector3_type V;
+  std::vector<prox::RigidBody<M> > body((size_t)std::max(n_bodies, 1));
+  std::vector<prox::ContactPoint<M> > c((size_t)n);
+  for (long long i = 0; i < n; ++i) {
+    float const* r = rows + 7 * i;
+    c[i].set_position(V::make(r[0], r[1], r[2]));
+    c[i].set_normal(V::make(r[3], r[4], r[5]));
+    c[i].set_depth(r[6]);
+    c[i].set_body_i(&body[bodies[2 * i]]);
+    c[i].set_body_j(&body[bodies[2 * i + 1]]);
+  }
+  std::sort(c.begin(), c.end());
+  c.erase(std::unique(c.begin(), c.end()), c.end());
+  *n_out = (long long)c.size();
+  for (size_t k = 0; k < c.size(); ++k) {
+    for (int j = 0; j < 3; ++j) {
+      out_rows[7 * k + j] = c[k].get_position()(j);
+      out_rows[7 * k + 3 + j] = c[k].get_normal()(j);
+    }
+    out_rows[7 * k + 6] = c[k].get_depth();
+    out_bodies[2 * k] = (unsigned)(c[k].get_body_i() - body.data());
+    out_bodies[2 * k + 1] = (unsigned)(c[k].get_body_j() - body.data());
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -40,6 +40,31 @@ def sorted_pairs(p: np.ndarray) -> np.ndarray:
     return p[o]
 
 
+def reduction_rows(rng, n_base=600, n_bodies=3):
+    """Contact rows (n, 7: p, n, depth) and bodies (n, 2) for the reduction."""
+    eps = np.float32(np.float32(np.finfo(np.float32).eps) * np.float32(10))
+    base = rng.uniform(-1, 1, (n_base, 7)).astype(np.float32)
+    bodies = rng.integers(0, n_bodies, (n_base, 2)).astype(np.uint32)
+    k = n_base // 2
+    src = rng.integers(0, n_base, k)
+    near = base[src] + (rng.integers(-4, 5, (k, 7)) * (np.float32(0.3) * eps)).astype(np.float32)
+    near[: k // 5] = base[src[: k // 5]]
+    chains = []
+    for c in range(20):
+        r0 = rng.uniform(-1, 1, 7).astype(np.float32)
+        steps = np.arange(6, dtype=np.float32)[:, None] * (np.float32(0.9) * eps)
+        chains.append(r0 + steps * np.array([0, 1, 0, 0, 0, 0, 0], np.float32))
+    chain = np.concatenate(chains)
+    chain_b = np.repeat(rng.integers(0, n_bodies, (20, 2)), 6, axis=0).astype(np.uint32)
+    rows = np.concatenate([base, near, chain]).astype(np.float32)
+    b = np.concatenate([bodies, bodies[src], chain_b]).astype(np.uint32)
+    z = rng.integers(0, len(rows), 40)
+    rows[z[:20], 1] = np.float32(0.0)
+    rows[z[20:], 1] = np.float32(-0.0)
+    perm = rng.permutation(len(rows))
+    return rows[perm], b[perm]
+
+
 def main():
     R = Reference()
     g = {}
@@ -107,6 +132,13 @@ def main():
     g["radius_xyz"] = np.concatenate([m.xyz for m in sb.meshes])
     g["radius_n"] = np.array([m.n_verts for m in sb.meshes], np.int64)
     g["radius_out"] = np.array([R.mesh_radius(m.xyz) for m in sb.meshes], np.float32)
+    # contact reduction: rows with near duplicates (offsets of whole multiples
+    # of 0.3 working precisions, inside and beyond it), exact copies, signed
+    # zeros and chains along p.y whose links are within the tolerance but
+    # whose ends are not, over three bodies
+    rr, rb = reduction_rows(np.random.default_rng(91))
+    g["reduce_rows"], g["reduce_bodies"] = rr, rb
+    g["reduce_out_rows"], g["reduce_out_bodies"] = R.reduce_contacts(rr, rb)
     np.savez_compressed(os.path.join(OUT, "reference_golden.npz"), **g)
     print("wrote", os.path.join(OUT, "reference_golden.npz"), os.path.getsize(os.path.join(OUT, "reference_golden.npz")),
           "bytes")

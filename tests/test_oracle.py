@@ -128,3 +128,28 @@ def test_broad_phase_oracle_against_reference_random(oracle, reference):
         want = reference.broad_pairs(pos, rad, 0)
         assert np.array_equal(oracle.broad_pairs(pos, rad), want)
         assert np.array_equal(reference.broad_pairs(pos, rad, 1), want)
+
+
+def _rows_equal(a, b):
+    # float == (a signed zero equals its opposite, as the reference's `<` treats it)
+    return a.shape == b.shape and bool(np.all(a == b))
+
+
+def test_contact_reduction_oracle_against_golden(oracle, golden):
+    rows, bodies = golden["reduce_rows"], golden["reduce_bodies"]
+    got_r, got_b, _ = oracle.reduce_contacts(rows, bodies)
+    assert _rows_equal(got_r, golden["reduce_out_rows"])
+    assert np.array_equal(got_b, golden["reduce_out_bodies"])
+    # the fixture exercises every case: removals, chains, signed zeros
+    assert len(golden["reduce_out_rows"]) < len(rows)
+
+
+def test_contact_reduction_oracle_against_reference_random(oracle, reference):
+    import sys
+    sys.path.insert(0, str(__import__("pathlib").Path(__file__).parent / "golden"))
+    from make_golden import reduction_rows
+    for seed, n_base, nb in ((1, 5, 1), (2, 40, 2), (3, 900, 4), (4, 3000, 1)):
+        rows, bodies = reduction_rows(np.random.default_rng(seed), n_base=n_base, n_bodies=nb)
+        want_r, want_b = reference.reduce_contacts(rows, bodies)
+        got_r, got_b, _ = oracle.reduce_contacts(rows, bodies)
+        assert _rows_equal(got_r, want_r) and np.array_equal(got_b, want_b)
