@@ -118,3 +118,20 @@ def test_reduce_scene_contacts(ctx, oracle):
     assert np.array_equal(out["cand"], rows["cand"][want_src])
     # the scene's own contacts and records are untouched (the adjoint still reads them)
     assert np.array_equal(ds.read_contacts().view(np.uint8), rows.view(np.uint8))
+
+
+def test_reduce_arguments_and_state_are_checked(ctx):
+    import ctypes as C
+    lib = kd.load_library()
+    n = C.c_int64()
+    rows = as_contacts(np.ones((3, 7), np.float32))
+    bodies = np.zeros((3, 2), np.uint32)
+    rp, bp = rows.ctypes.data_as(C.c_void_p), bodies.ctypes.data_as(C.c_void_p)
+    assert lib.kdop_reduce_contact_rows(None, rp, bp, 3, rp, None, 3, C.byref(n)) == kd.lib.ERR_INVALID
+    assert lib.kdop_reduce_contact_rows(ctx.h, rp, bp, -1, rp, None, 3, C.byref(n)) == kd.lib.ERR_INVALID
+    assert lib.kdop_reduce_contact_rows(ctx.h, None, bp, 3, rp, None, 3, C.byref(n)) == kd.lib.ERR_INVALID
+    assert lib.kdop_reduce_contact_rows(ctx.h, rp, bp, 3, rp, None, 3, None) == kd.lib.ERR_INVALID
+    sc = scenes.small_batch(n_pairs=2, seed=3)
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    with pytest.raises(kd.KdopError):
+        ds.reduce_contacts()  # before kdop_contacts
