@@ -241,10 +241,11 @@ int kdop_set_capacity(kdop_scene* scene, int64_t candidates, int64_t contacts, i
 
 /* Tandem traversal that allocates no device memory.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc while they
- * run -- code recording a caller-owned stream into a CUDA graph (device
- * allocation is not allowed during capture), simulators that keep a fixed
- * device-memory budget or arena for the whole run, and real-time loops that
- * must not risk an allocation failure mid-step.
+ * run -- a plugin inside a host application whose own allocator must own
+ * every byte of device memory, simulators that reserve a fixed
+ * device-memory budget or arena once at start-up, and real-time loops that
+ * must not risk an allocation failure (or an allocator's device-wide
+ * synchronisation) in the middle of a step.
  *
  * The caller passes device memory only: pairs (n_pairs * 2 mesh indices),
  * candidates (3 * cap uint32: tets of A | tets of B | pair indices; tet

@@ -1,6 +1,8 @@
 """kdop_traverse_noalloc: the traversal entry point that allocates no device
-memory, for callers that cannot call cudaMalloc while they run (a stream being
-recorded into a CUDA graph, a fixed device-memory budget, a real-time step).
+memory, for callers that cannot call cudaMalloc while they run (a plugin whose
+host application's allocator owns all device memory, a simulator with a fixed
+device-memory budget reserved at start-up, a real-time step that must not
+risk an allocation failure).
 
 The caller owns every buffer (here torch allocates them, in the test, before
 the call); the entry point keeps its scratch in a static device array.  Its
