@@ -164,6 +164,7 @@ int kdop_ctx_create(int device, kdop_ctx** out) {
 
 static void ctx_free(kdop_ctx* ctx) {
   cudaSetDevice(ctx->device);
+  if (ctx->scratch) cudaFree(ctx->scratch);  // waits for the device
   if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -1024,33 +1025,54 @@ int kdop_read_contacts(kdop_scene* s, kdop_contact* rows, int64_t cap, int64_t* 
 }
 
 // ---- contact reduction (prox_collision_detection.h:341-350) ----
-// Reduces n device rows with their device bodies into scratch, then copies
-// the kept rows (and bodies) to the caller's buffers (host or device).
-static int reduce_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint2* bodies, int64_t n, kdop_contact* out,
-                       uint32_t* out_bodies, int64_t cap, int64_t* n_out) {
-  const size_t wb = (kdop::reduce_work_bytes(n) + 255) & ~(size_t)255;
-  const size_t rb = ((size_t)std::max<int64_t>(n, 1) * sizeof(kdop_contact) + 255) & ~(size_t)255;
-  char* buf = nullptr;
-  KDOP_CUDA(ctx, cudaMalloc((void**)&buf, wb + rb + (size_t)std::max<int64_t>(n, 1) * sizeof(uint2)));
+static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// The context's grow-only scratch, at least `bytes` long.  Calls on a context
+// are serial, so one buffer serves every reduction; growing frees the old
+// buffer (cudaFree waits for the work that used it).
+static cudaError_t ctx_scratch(kdop_ctx* ctx, size_t bytes, char** p) {
+  if (bytes > ctx->scratch_bytes) {
+    if (ctx->scratch) cudaFree(ctx->scratch);
+    ctx->scratch = nullptr;
+    ctx->scratch_bytes = 0;
+    cudaError_t e = cudaMalloc((void**)&ctx->scratch, bytes);
+    if (e != cudaSuccess) return e;
+    ctx->scratch_bytes = bytes;
+  }
+  *p = ctx->scratch;
+  return cudaSuccess;
+}
+
+// Bytes reduce_rows needs for n rows: the sort's work, then the kept rows and
+// their bodies.
+static size_t reduce_rows_bytes(int64_t n) {
+  const size_t m = (size_t)std::max<int64_t>(n, 1);
+  return align256(kdop::reduce_work_bytes(n)) + align256(m * sizeof(kdop_contact)) + align256(m * sizeof(uint2));
+}
+
+// Reduces n device rows with their device bodies in `buf` (reduce_rows_bytes(n)
+// bytes), then copies the kept rows (and bodies) to the caller's buffers
+// (host or device).
+static int reduce_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint2* bodies, int64_t n, char* buf,
+                       kdop_contact* out, uint32_t* out_bodies, int64_t cap, int64_t* n_out) {
+  const size_t m = (size_t)std::max<int64_t>(n, 1);
+  const size_t wb = align256(kdop::reduce_work_bytes(n));
+  const size_t rb = align256(m * sizeof(kdop_contact));
   kdop_contact* kept_rows = reinterpret_cast<kdop_contact*>(buf + wb);
   uint2* kept_bodies = reinterpret_cast<uint2*>(buf + wb + rb);
   int64_t kept = 0;
   cudaError_t e = kdop::reduce_contact_rows(ctx, rows, bodies, n, buf, kept_rows, kept_bodies, &kept);
-  int rc = KDOP_OK;
   *n_out = kept;
-  if (e != cudaSuccess) {
-    rc = cuda_fail(ctx, e, "reduce_contact_rows");
-  } else if (kept > cap) {
-    rc = fail(ctx, KDOP_ERR_CAPACITY, "reduced contact buffer too small");
-  } else if (kept > 0) {
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "reduce_contact_rows");
+  if (kept > cap) return fail(ctx, KDOP_ERR_CAPACITY, "reduced contact buffer too small");
+  if (kept > 0) {
     e = cudaMemcpyAsync(out, kept_rows, (size_t)kept * sizeof(kdop_contact), cudaMemcpyDefault, ctx->stream);
     if (e == cudaSuccess && out_bodies)
       e = cudaMemcpyAsync(out_bodies, kept_bodies, (size_t)kept * sizeof(uint2), cudaMemcpyDefault, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "reduced contacts copy");
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "reduced contacts copy");
   }
-  cudaFree(buf);
-  return rc;
+  return KDOP_OK;
 }
 
 int kdop_reduce_contact_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint32_t* bodies, int64_t n,
@@ -1060,18 +1082,20 @@ int kdop_reduce_contact_rows(kdop_ctx* ctx, const kdop_contact* rows, const uint
   *n_out = 0;
   if (n == 0) return KDOP_OK;
   cudaSetDevice(ctx->device);
-  const size_t rb = ((size_t)n * sizeof(kdop_contact) + 255) & ~(size_t)255;
+  // staged input (rows, bodies), then the reduction's own scratch
+  const size_t rb = align256((size_t)n * sizeof(kdop_contact));
+  const size_t bb = align256((size_t)n * sizeof(uint2));
   char* in = nullptr;
-  KDOP_CUDA(ctx, cudaMalloc((void**)&in, rb + (size_t)n * sizeof(uint2)));
+  KDOP_CUDA(ctx, ctx_scratch(ctx, rb + bb + reduce_rows_bytes(n), &in));
   cudaError_t e = cudaMemcpyAsync(in, rows, (size_t)n * sizeof(kdop_contact), cudaMemcpyDefault, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(in + rb, bodies, (size_t)n * sizeof(uint2), cudaMemcpyDefault, ctx->stream);
-  int rc = e != cudaSuccess ? cuda_fail(ctx, e, "reduce input copy")
-                            : reduce_rows(ctx, reinterpret_cast<kdop_contact*>(in), reinterpret_cast<uint2*>(in + rb),
-                                          n, out, out_bodies, cap, n_out);
-  cudaStreamSynchronize(ctx->stream);
-  cudaFree(in);
-  return rc;
+  if (e != cudaSuccess) {
+    cudaStreamSynchronize(ctx->stream);  // a started copy may still read the caller's rows
+    return cuda_fail(ctx, e, "reduce input copy");
+  }
+  return reduce_rows(ctx, reinterpret_cast<kdop_contact*>(in), reinterpret_cast<uint2*>(in + rb), n, in + rb + bb,
+                     out, out_bodies, cap, n_out);
 }
 
 int kdop_reduce_contacts(kdop_scene* s, kdop_contact* out, uint32_t* out_bodies, int64_t cap, int64_t* n_out) {
@@ -1083,14 +1107,14 @@ int kdop_reduce_contacts(kdop_scene* s, kdop_contact* out, uint32_t* out_bodies,
   const int64_t n = std::min<int64_t>(st.n_contacts, s->contact_cap);
   *n_out = 0;
   if (n <= 0) return KDOP_OK;
-  uint2* bodies = nullptr;
-  KDOP_CUDA(s->ctx, cudaMalloc((void**)&bodies, (size_t)n * sizeof(uint2)));
+  // the rows' bodies, then the reduction's own scratch
+  const size_t bb = align256((size_t)n * sizeof(uint2));
+  char* buf = nullptr;
+  KDOP_CUDA(s->ctx, ctx_scratch(s->ctx, bb + reduce_rows_bytes(n), &buf));
+  uint2* bodies = reinterpret_cast<uint2*>(buf);
   cudaError_t e = kdop::scene_contact_bodies(s, n, bodies);
-  rc = e != cudaSuccess ? cuda_fail(s->ctx, e, "scene_contact_bodies")
-                        : reduce_rows(s->ctx, s->contacts, bodies, n, out, out_bodies, cap, n_out);
-  cudaStreamSynchronize(s->ctx->stream);
-  cudaFree(bodies);
-  return rc;
+  if (e != cudaSuccess) return cuda_fail(s->ctx, e, "scene_contact_bodies");
+  return reduce_rows(s->ctx, s->contacts, bodies, n, buf + bb, out, out_bodies, cap, n_out);
 }
 
 int kdop_contacts_adjoint(kdop_scene* s, const float* dd, const float* dn, float* grad, int memory) {

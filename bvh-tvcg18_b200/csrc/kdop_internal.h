@@ -82,6 +82,9 @@ struct kdop_ctx {
   bool destroy_pending = false;
   // autotuned traversal options keyed by (K, size class)
   std::map<std::pair<int, int>, kdop_traverse_opts> tuned;
+  // grow-only device scratch of the contact reduction, freed with the context
+  char* scratch = nullptr;
+  size_t scratch_bytes = 0;
 };
 
 struct kdop_scene {

@@ -298,7 +298,9 @@ int kdop_read_contacts(kdop_scene* scene, kdop_contact* rows, int64_t cap_rows, 
  * when that exceeds cap.  Rows whose nine key fields all compare equal keep
  * their input order (std::sort leaves it unspecified; such rows can differ
  * only in the sign of a zero and in `cand`, and all but the first are
- * dropped).  Synchronises.
+ * dropped).  Synchronises.  The sort's scratch is device memory the context
+ * keeps for later calls (allocated when a call needs more than it holds,
+ * freed by kdop_ctx_destroy).
  *
  * kdop_reduce_contacts: the scene's contacts of the last kdop_contacts, the
  * bodies of a row being the meshes (A, B) of its candidate's pair.
