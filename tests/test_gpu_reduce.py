@@ -79,6 +79,22 @@ def test_reduce_rows_edge_cases(ctx):
     assert not dst.view(np.uint8).any()
 
 
+def test_reduce_scratch_reused_across_sizes(oracle):
+    """The sort scratch lives in the context: a fresh context reduces sets that
+    grow, shrink and grow again, each equal to the oracle's result."""
+    c = kd.Context(0)
+    try:
+        for seed, n_base, nb in [(21, 20000, 4), (22, 3, 1), (23, 60000, 9), (24, 500, 2), (25, 60000, 9)]:
+            rows, bodies = reduction_rows(np.random.default_rng(seed), n_base=n_base, n_bodies=nb)
+            want_r, want_b, want_src = oracle.reduce_contacts(rows, bodies)
+            out, ob = c.reduce_contact_rows(as_contacts(rows), bodies)
+            assert np.array_equal(ob, want_b), seed
+            assert np.all(as_rows7(out) == want_r), seed
+            assert np.array_equal(out["cand"], want_src), seed
+    finally:
+        c.close()
+
+
 def test_reduce_rows_device_buffers(ctx, oracle):
     torch = pytest.importorskip("torch")
     rows, bodies = reduction_rows(np.random.default_rng(8), n_base=3000, n_bodies=5)
