@@ -399,8 +399,16 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         const int src = ge * Q + TQ;
         const uint32_t wA0 = __shfl_sync(0xffffffffu, t0, src);
         const uint32_t wA1 = __shfl_sync(0xffffffffu, t1, src);
-        const uint32_t wB0 = __shfl_sync(0xffffffffu, t2, src);
-        const uint32_t wB1 = __shfl_sync(0xffffffffu, t3, src);
+        uint32_t wB0, wB1;
+        if (Q == 2) {
+          // lane gq only handles child gq of B (see below): the topology lane
+          // keeps its own word, the other lane gets the other child's
+          const uint32_t wo = __shfl_sync(0xffffffffu, TQ ? t2 : t3, src);
+          wB0 = wB1 = (gq == TQ) ? (TQ ? t3 : t2) : wo;
+        } else {
+          wB0 = __shfl_sync(0xffffffffu, t2, src);
+          wB1 = __shfl_sync(0xffffffffu, t3, src);
+        }
         if (valid) {
           if (gq == 0) tests32 += (singleA ? 1u : 2u) * (singleB ? 1u : 2u);
           // the lane's child pairs c = gq + Q r (c = 2 i + k: child i of A,
