@@ -457,19 +457,27 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         }
       }
     }
-    // ---- pushes: ballot prefix sum, then deque (or the global queue) ----
+    // ---- pushes: deque (or the global queue), slot-major: every lane's
+    // slot-0 push, then every slot-1 push, ..., so that the lanes of one store
+    // instruction write consecutive positions (one ballot per slot) ----
     {
-      int tot_p = 0, off_p = 0;
-      warp_prefix<CBITS>(__popc(push_mask), lt_mask, tot_p, off_p);
+      unsigned pm[SLOTS];
+      int pbase[SLOTS];
+      int tot_p = 0;
+#pragma unroll
+      for (int k = 0; k < SLOTS; ++k) {
+        pm[k] = __ballot_sync(0xffffffffu, (push_mask >> k) & 1u);
+        pbase[k] = tot_p;
+        tot_p += __popc(pm[k]);
+      }
       if (tot_p) {
         if (top - bot + tot_p <= CAP) {
-          int at = top + off_p;
 #pragma unroll
           for (int k = 0; k < SLOTS; ++k) {
             if (push_mask & (1u << k)) {
-              sAB[at & MASK] = make_uint2(pushA[k], pushB[k]);
-              sP[at & MASK] = slotP[k];
-              ++at;
+              const int at = (top + pbase[k] + __popc(pm[k] & lt_mask)) & MASK;
+              sAB[at] = make_uint2(pushA[k], pushB[k]);
+              sP[at] = slotP[k];
             }
           }
           top += tot_p;
@@ -483,23 +491,18 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
           if (room < tot_p && lane == 0) atomicOr(&ctl->error, DEV_ERR_QUEUE_FULL);
           if (room > 0 && lane == 0) atomicAdd(&ctl->work, room);
           __syncwarp();
-          unsigned slot = t0 + (unsigned)off_p;
 #pragma unroll
           for (int k = 0; k < SLOTS; ++k) {
-            if (push_mask & (1u << k)) {
-              if (slot < t0 + (unsigned)room) a.q_items[slot] = make_uint4(pushA[k], pushB[k], slotP[k], 0u);
-              ++slot;
-            }
+            const unsigned slot = t0 + (unsigned)(pbase[k] + __popc(pm[k] & lt_mask));
+            if ((push_mask & (1u << k)) && slot < t0 + (unsigned)room)
+              a.q_items[slot] = make_uint4(pushA[k], pushB[k], slotP[k], 0u);
           }
           __threadfence();
           __syncwarp();
-          slot = t0 + (unsigned)off_p;
 #pragma unroll
           for (int k = 0; k < SLOTS; ++k) {
-            if (push_mask & (1u << k)) {
-              if (slot < t0 + (unsigned)room) atomicExch(&a.q_tags[slot], 1u);
-              ++slot;
-            }
+            const unsigned slot = t0 + (unsigned)(pbase[k] + __popc(pm[k] & lt_mask));
+            if ((push_mask & (1u << k)) && slot < t0 + (unsigned)room) atomicExch(&a.q_tags[slot], 1u);
           }
         }
       }
