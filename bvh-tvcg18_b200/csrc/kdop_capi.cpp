@@ -224,7 +224,7 @@ static void scene_free(kdop_scene* s) {
   dfree(s, &s->phase_dev, 1);
   dfree(s, &s->pairs, s->pairs_cap);
   dfree(s, &s->pair_order, s->pairs_cap);
-  dfree(s, &s->cand, 4 * s->cand_cap);
+  dfree(s, &s->cand, kdop::kCandCols * s->cand_cap);
   dfree(s, &s->contacts, s->contact_cap);
   dfree(s, &s->records, s->cand_cap);
   dfree(s, &s->q_items, s->queue_cap);
@@ -265,11 +265,11 @@ static void drop_graph(kdop_scene* s) {
 static int grow_candidates(kdop_scene* s, int64_t n) {
   if (n <= s->cand_cap) return KDOP_OK;
   drop_graph(s);
-  dfree(s, &s->cand, 4 * s->cand_cap);
+  dfree(s, &s->cand, kdop::kCandCols * s->cand_cap);
   dfree(s, &s->records, s->cand_cap);
   s->cand_cap = 0;
   if (n >= (int64_t)0xFFFFFFF0ll) return fail(s->ctx, KDOP_ERR_CAPACITY, "candidate capacity above 2^32");
-  KDOP_CUDA(s->ctx, dalloc(s, &s->cand, 4 * n));
+  KDOP_CUDA(s->ctx, dalloc(s, &s->cand, kdop::kCandCols * n));
   KDOP_CUDA(s->ctx, dalloc(s, &s->records, n));
   s->cand_cap = n;
   return KDOP_OK;
@@ -925,7 +925,7 @@ int kdop_set_capacity(kdop_scene* s, int64_t candidates, int64_t contacts, int64
   int rc = KDOP_OK;
   if (candidates || contacts || queue) drop_graph(s);
   if (candidates) {
-    dfree(s, &s->cand, 4 * s->cand_cap);
+    dfree(s, &s->cand, kdop::kCandCols * s->cand_cap);
     dfree(s, &s->records, s->cand_cap);
     s->cand_cap = 0;
     rc = grow_candidates(s, candidates);

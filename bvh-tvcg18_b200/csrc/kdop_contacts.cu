@@ -143,6 +143,7 @@ struct ContactArgs {
   const uint32_t* candB;
   const uint32_t* candP;
   uint32_t* surv;  // candidates past the pre-filter (n_surv of them)
+  uint32_t* mid;   // candidates past the face axes of the SAT test (n_mid of them)
   unsigned cand_cap;
   const uint4* __restrict__ tets;
   const uint8_t* __restrict__ surf;
@@ -172,48 +173,89 @@ __device__ __forceinline__ bool face_pair_ok(int fa, int fb, uint32_t sa, uint32
   return true;
 }
 
-// Pass 1: thread per candidate.  A pair that fails the SAT test or has no
-// admissible face pair gets its empty record here; the others are listed.
+// Tets ta and tb of a candidate, posed.
+__device__ __forceinline__ void candidate_tets(const ContactArgs& a, uint32_t ta, uint32_t tb, f3* A, f3* B) {
+  const uint4 qa = __ldg(a.tets + ta), qb = __ldg(a.tets + tb);
+  A[0] = world_vertex(a.vs, qa.x);
+  A[1] = world_vertex(a.vs, qa.y);
+  A[2] = world_vertex(a.vs, qa.z);
+  A[3] = world_vertex(a.vs, qa.w);
+  B[0] = world_vertex(a.vs, qb.x);
+  B[1] = world_vertex(a.vs, qb.y);
+  B[2] = world_vertex(a.vs, qb.z);
+  B[3] = world_vertex(a.vs, qb.w);
+}
+
+// Appends the warp's kept candidates to a list (one atomic per warp).
+__device__ __forceinline__ void warp_append(bool keep, unsigned ci, unsigned* counter, uint32_t* list, int lane) {
+  const unsigned m = __ballot_sync(0xffffffffu, keep);
+  if (m) {
+    unsigned at = 0;
+    if (lane == 0) at = atomicAdd(counter, (unsigned)__popc(m));
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (keep) list[at + __popc(m & ((1u << lane) - 1u))] = ci;
+  }
+}
+
+// Pass 1a: thread per candidate, the surface check and the 8 face axes of the
+// SAT test.  A pair they reject gets its empty record here; the others are
+// listed for pass 1b, so that the 36 edge axes run on dense warps.  The SAT
+// verdict is an OR over all 44 axes, so splitting the axes leaves it as it is.
 __global__ void __launch_bounds__(256) contacts_filter_kernel(ContactArgs a) {
   const int lane = threadIdx.x & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
   const unsigned n_cand = min(*(volatile unsigned*)&a.ctl->n_cand, a.cand_cap);
   const unsigned stride = gridDim.x * blockDim.x;
   for (unsigned base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_cand; base += stride) {
     const unsigned ci = base + lane;
     bool keep = false;
     if (ci < n_cand) {
-      uint32_t ta = a.candA[ci], tb = a.candB[ci];
-      uint32_t sa = a.surf[ta], sb = a.surf[tb];
-      if (sa != 0u && sb != 0u) {
-        uint4 qa = __ldg(a.tets + ta), qb = __ldg(a.tets + tb);
-        f3 A[4] = {world_vertex(a.vs, qa.x), world_vertex(a.vs, qa.y), world_vertex(a.vs, qa.z),
-                   world_vertex(a.vs, qa.w)};
-        f3 B[4] = {world_vertex(a.vs, qb.x), world_vertex(a.vs, qb.y), world_vertex(a.vs, qb.z),
-                   world_vertex(a.vs, qb.w)};
+      const uint32_t ta = a.candA[ci], tb = a.candB[ci];
+      if (a.surf[ta] != 0u && a.surf[tb] != 0u) {
+        f3 A[4], B[4];
+        candidate_tets(a, ta, tb, A, B);
         bool sep = false;
-        for (int t = 0; t < 44 && !sep; ++t) sep = sat_test(t, A, B);
-        if (!sep) {
-          UPlane PA[4], PB[4];
-#pragma unroll
-          for (int f = 0; f < 4; ++f) {
-            PA[f] = unscaled_plane(A[c_face[f][0]], A[c_face[f][1]], A[c_face[f][2]]);
-            PB[f] = unscaled_plane(B[c_face[f][0]], B[c_face[f][1]], B[c_face[f][2]]);
-          }
-          float test;
-          f3 nA;
-          for (int l = 0; l < 16 && !keep; ++l) keep = face_pair_ok(l >> 2, l & 3, sa, sb, PA, PB, A, B, test, nA);
-        }
+        for (int t = 0; t < 8 && !sep; ++t) sep = sat_test(t, A, B);
+        keep = !sep;
       }
       if (!keep) a.rec[ci] = make_int4(-1, -1, 0, 0);
     }
-    unsigned m = __ballot_sync(0xffffffffu, keep);
-    if (m) {
-      unsigned at = 0;
-      if (lane == 0) at = atomicAdd(&a.ctl->n_surv, (unsigned)__popc(m));
-      at = __shfl_sync(0xffffffffu, at, 0);
-      if (keep) a.surv[at + __popc(m & lt_mask)] = ci;
+    warp_append(keep, ci, &a.ctl->n_mid, a.mid, lane);
+  }
+}
+
+// Pass 1b: thread per candidate past the face axes: the 36 edge axes of the
+// SAT test, then the search for an admissible face pair.  A pair that fails
+// gets its empty record here; the others are listed for pass 2.
+__global__ void __launch_bounds__(256) contacts_edge_kernel(ContactArgs a) {
+  const int lane = threadIdx.x & 31;
+  const unsigned n_mid = *(volatile unsigned*)&a.ctl->n_mid;
+  const unsigned stride = gridDim.x * blockDim.x;
+  for (unsigned base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n_mid; base += stride) {
+    const unsigned k = base + lane;
+    bool keep = false;
+    unsigned ci = 0;
+    if (k < n_mid) {
+      ci = a.mid[k];
+      const uint32_t ta = a.candA[ci], tb = a.candB[ci];
+      const uint32_t sa = a.surf[ta], sb = a.surf[tb];
+      f3 A[4], B[4];
+      candidate_tets(a, ta, tb, A, B);
+      bool sep = false;
+      for (int t = 8; t < 44 && !sep; ++t) sep = sat_test(t, A, B);
+      if (!sep) {
+        UPlane PA[4], PB[4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          PA[f] = unscaled_plane(A[c_face[f][0]], A[c_face[f][1]], A[c_face[f][2]]);
+          PB[f] = unscaled_plane(B[c_face[f][0]], B[c_face[f][1]], B[c_face[f][2]]);
+        }
+        float test;
+        f3 nA;
+        for (int l = 0; l < 16 && !keep; ++l) keep = face_pair_ok(l >> 2, l & 3, sa, sb, PA, PB, A, B, test, nA);
+      }
+      if (!keep) a.rec[ci] = make_int4(-1, -1, 0, 0);
     }
+    warp_append(keep, ci, &a.ctl->n_surv, a.surv, lane);
   }
 }
 
@@ -481,6 +523,7 @@ __global__ void contacts_reset_kernel(TravCtl* c) {
   if (threadIdx.x == 0) {
     c->n_contacts = 0;
     c->n_surv = 0;
+    c->n_mid = 0;
   }
 }
 
@@ -503,6 +546,7 @@ cudaError_t launch_contacts(kdop_scene* s) {
   a.candB = s->cand + s->cand_cap;
   a.candP = s->cand + 2 * s->cand_cap;
   a.surv = s->cand + 3 * s->cand_cap;
+  a.mid = s->cand + 4 * s->cand_cap;
   a.cand_cap = (unsigned)s->cand_cap;
   a.tets = s->tets;
   a.surf = s->surf;
@@ -514,8 +558,9 @@ cudaError_t launch_contacts(kdop_scene* s) {
   contacts_reset_kernel<<<1, 32, 0, s->ctx->stream>>>(s->ctl);
   unsigned grid = (unsigned)s->ctx->sm_count * 8u;
   contacts_filter_kernel<<<grid, 256, 0, s->ctx->stream>>>(a);
+  contacts_edge_kernel<<<grid, 256, 0, s->ctx->stream>>>(a);
   contacts_thread_kernel<<<grid * 2, 128, 0, s->ctx->stream>>>(a);
-  s->ctx->launches += 3;
+  s->ctx->launches += 4;
   return cudaGetLastError();
 }
 

@@ -22,6 +22,9 @@ struct DirTable {
   float d[13][3];
 };
 
+// Columns of a scene's candidate buffer (each cand_cap uint32).
+constexpr int kCandCols = 5;
+
 // Device-side control block of one traversal (+ contact generation).  The counters that every warp updates or polls
 // while the traversal runs sit on 128-byte lines of their own, so that atomics
 // and polls on one do not queue behind traffic on another in the same L2 slice.
@@ -34,7 +37,8 @@ struct TravCtl {
   unsigned int pair_base;            // pair index of the first root pair
   unsigned int max_stack;            // deepest warp stack seen
   unsigned int n_surv;               // candidates past the contact pre-filter
-  unsigned int pad0[22];
+  unsigned int n_mid;                // candidates past the face axes of the SAT test
+  unsigned int pad0[21];
   unsigned int n_cand;               // candidates emitted (may exceed capacity)
   unsigned int pad1[31];
   unsigned int init_head;            // root pairs claimed
@@ -117,7 +121,8 @@ struct kdop_scene {
   uint2* pairs = nullptr;
   uint32_t* pair_order = nullptr;  // pair indices by decreasing size (tets of A + tets of B)
   int64_t pairs_cap = 0;
-  uint32_t* cand = nullptr;  // 4 * cand_cap: A tets | B tets | pair ids | pre-filter survivors
+  uint32_t* cand = nullptr;  // kCandCols * cand_cap: A tets | B tets | pair ids | pre-filter survivors |
+                             // candidates past the face axes of the SAT test
   int64_t cand_cap = 0;
   kdop_contact* contacts = nullptr;
   int4* records = nullptr;  // per candidate: faces, candidate codes, count, first contact
