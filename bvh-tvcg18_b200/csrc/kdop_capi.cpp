@@ -212,6 +212,7 @@ static void scene_free(kdop_scene* s) {
   s->graph = nullptr;
   dfree(s, &s->rest, s->nv);
   dfree(s, &s->world, s->nv);
+  dfree(s, &s->posed, s->nv);
   dfree(s, &s->tets, s->nt);
   dfree(s, &s->surf, s->nt);
   dfree(s, &s->nodes, s->nn * s->NW);
@@ -426,6 +427,7 @@ int kdop_scene_create_ex(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_des
   }
     SC_TRY(dalloc(s, &s->rest, nv));
     SC_TRY(dalloc(s, &s->world, nv));
+    SC_TRY(dalloc(s, &s->posed, nv));
     SC_TRY(dalloc(s, &s->tets, nt));
     SC_TRY(dalloc(s, &s->surf, nt));
     SC_TRY(dalloc(s, &s->nodes, s->nn * s->NW));

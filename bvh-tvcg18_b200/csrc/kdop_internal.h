@@ -105,6 +105,7 @@ struct kdop_scene {
   // device arrays
   float4* rest = nullptr;
   float4* world = nullptr;
+  float4* posed = nullptr;  // world positions a pose / deform refit computes before its leaf pass
   uint4* tets = nullptr;  // global vertex indices
   uint8_t* surf = nullptr;
   float4* nodes = nullptr;

@@ -12,10 +12,13 @@
 // its four vertices once and projects them on all K/2 directions; an internal
 // node reads its children's twin record (2 NW consecutive float4, independent
 // loads in flight together).  Two sibling threads write the interleaved
-// chunks of one twin, so every store instruction fills whole 32-byte sectors.  Leaves transform their vertices on the fly when the scene is in
-// pose or deform mode (narrow_update_kdop_bvh.h:154-165 fused into the leaf
-// pass, so no world-vertex array is written).  The upper levels, too small to
-// fill the GPU, are refitted by one block that walks them with block barriers.
+// chunks of one twin, so every store instruction fills whole 32-byte sectors.
+// In pose or deform mode the refit first poses every vertex once
+// (narrow_update_kdop_bvh.h:154-165 on the device, in the same call and the
+// same graph) into a scene-owned array the leaves read: posing inside the leaf
+// pass would transform each vertex once per tet that uses it (about 24 times
+// in a lattice).  The upper levels, too small to fill the GPU, are refitted by
+// one block that walks them with block barriers.
 #include "kdop_device.cuh"
 
 namespace kdop {
@@ -217,6 +220,14 @@ static const int64_t* level_off_dev(kdop_scene* s) {
 template <int K>
 static cudaError_t refit_impl(kdop_scene* s, int mode) {
   VertexSource vs = vertex_source(s, mode);
+  if (mode != KDOP_REFIT_VERTICES && s->nv > 0) {
+    // pose (and deform) every vertex once; the leaves then read world
+    // positions instead of transforming each vertex once per tet using it
+    world_kernel<<<(unsigned)((s->nv + 255) / 256), 256, 0, s->ctx->stream>>>(s->nv, vs, s->posed);
+    s->ctx->launches++;
+    vs = vertex_source(s, KDOP_REFIT_VERTICES);
+    vs.world = s->posed;
+  }
   const int64_t small = 4096;  // nodes of a level refitted by the single-block kernel
   int levels = (int)s->level_off.size() - 1;
   if (levels <= 0) return cudaSuccess;

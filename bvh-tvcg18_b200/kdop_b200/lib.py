@@ -3,7 +3,7 @@
 Mirrors the reference's kDOP interface for one simulation step
 (SIMULATION/KDOP/KDOP/include): a DeviceScene replaces mesh_reorder +
 make_tree for a set of meshes, refit() replaces refit_tree (with the rigid
-transform of narrow_update_kdop_bvh.h fused), traverse() replaces
+transform of narrow_update_kdop_bvh.h done on the device), traverse() replaces
 tandem_traversal over a pool of TestPairs, and contacts() returns what the
 reference reports through ContactsCallback (point, normal, depth).
 """

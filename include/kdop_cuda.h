@@ -12,7 +12,7 @@
  *   kdop::refit_tree<V,K,T>(tree, mesh, X, Y, Z, tag)
  *       kdop_refit_tree.h:120-162 (CPU), cl/kdop_cl_refit_tree.h:53-283 (OpenCL)
  *       with the rigid transform of narrow_update_kdop_bvh.h:154-165 and
- *       narrow_cl_transform_vertices.cl:5-45 fused in
+ *       narrow_cl_transform_vertices.cl:5-45 done on the device in the same call
  *         -> kdop_set_vertices / kdop_set_poses / kdop_refit
  *   kdop::tandem_traversal<V,K,T>(std::vector<TestPair>&, tag)
  *       kdop_tandem_traversal.h:160-226 (CPU),
@@ -141,8 +141,8 @@ int kdop_set_deformation(kdop_scene* scene, float amp, float w, float phase);
 
 typedef enum {
   KDOP_REFIT_VERTICES = 0, /* refit from the world positions of kdop_set_vertices */
-  KDOP_REFIT_POSE = 1,     /* world = rotate(q, rest) + p, fused into the leaf pass */
-  KDOP_REFIT_DEFORM = 2    /* world = rotate(q, rest + displacement) + p, fused */
+  KDOP_REFIT_POSE = 1,     /* world = rotate(q, rest) + p, computed by the refit on the device */
+  KDOP_REFIT_DEFORM = 2    /* world = rotate(q, rest + displacement) + p, likewise */
 } kdop_refit_mode;
 /* Bottom-up refit of every tree of the scene; the mode also fixes how the
  * contact kernels obtain world positions until the next refit. */
