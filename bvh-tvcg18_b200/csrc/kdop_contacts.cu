@@ -537,6 +537,11 @@ static VertexSource vsrc(kdop_scene* s) {
   vs.deform.w = s->w;
   vs.deform.phase = s->phase_dev;
   vs.mode = s->refit_mode < 0 ? 0 : s->refit_mode;
+  if (vs.mode != KDOP_REFIT_VERTICES) {
+    // the world positions the last pose / deform refit computed (and traversed)
+    vs.mode = KDOP_REFIT_VERTICES;
+    vs.world = s->posed;
+  }
   return vs;
 }
 

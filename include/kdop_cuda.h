@@ -279,7 +279,11 @@ typedef struct {
 
 /* MOST_OPPOSING_SURFACES contacts
  * (geometry_contacts_tetrahedron_tetrahedron.h:1313-1345) of every candidate
- * of the last traversal.  Asynchronous. */
+ * of the last traversal, from the vertex positions of the last refit: the
+ * posed (and deformed) positions it computed in KDOP_REFIT_POSE /
+ * KDOP_REFIT_DEFORM mode, the kdop_set_vertices positions in
+ * KDOP_REFIT_VERTICES mode.  kdop_contacts_adjoint differentiates with
+ * respect to the same positions.  Asynchronous. */
 int kdop_contacts(kdop_scene* scene);
 /* Contacts grouped by candidate (rows of one candidate are contiguous, in the
  * reference's reporting order).  `rows` may be host or device memory (a
