@@ -13,14 +13,18 @@
 //      all candidates, points projected on the mid plane, near-duplicates
 //      (max-norm < 10 FLT_EPSILON) dropped, reported in order (:622-681).
 //
-// Two passes, a thread per candidate tet pair in each.  The first runs steps
-// 1 and 2 up to the first separating axis or the first admissible face pair
-// (almost all leaf pairs of a deep overlap stop there: no contact) and lists
-// the pairs that go on; the second runs step 2's argmin and step 3 for the
-// listed pairs in the reference's order (face pairs, then the 56 candidates
-// in generation order), so the reported rows and every value equal the
-// reference's FP32 results.  Both passes evaluate the same functions on the
-// same inputs, so their decisions agree.  (A warp-per-pair form, lanes over
+// Three passes, a thread per candidate tet pair in each.  The first two run
+// steps 1 and 2 up to the first separating axis or the first admissible face
+// pair (almost all leaf pairs of a deep overlap stop there: no contact) --
+// the 8 face axes of the SAT test in the first, the 36 edge axes and the
+// face-pair search in the second, on the pairs the first lists densely -- and
+// list the pairs that go on; the third runs step 2's argmin and step 3 for
+// the listed pairs in the reference's order (face pairs, then the 56
+// candidates in generation order), so the reported rows and every value equal
+// the reference's FP32 results.  All passes evaluate the same functions on
+// the same inputs, so their decisions agree.  Vertex positions are the world
+// positions the last refit used (after a pose / deform refit, the array it
+// computed).  (A warp-per-pair form, lanes over
 // SAT axes, face pairs and candidates with ballots keeping the order, took
 // 1.5x longer on contact-rich pairs: most phases kept few lanes busy.)
 #include "kdop_device.cuh"
