@@ -132,6 +132,40 @@ def test_touching_pairs_contacts_bit_exact(ctx, oracle, golden, seed):
                        B, ref_pairs)
 
 
+def test_contacts_use_the_positions_of_the_last_refit(ctx):
+    """After a pose refit, contacts (and the adjoint) read the world positions
+    that refit computed -- the ones the traversal saw -- so a pose change
+    between refit and kdop_contacts does not mix two poses; the same rows come
+    back as from the world positions uploaded and refitted in vertex mode."""
+    sc = scenes.touching_pair(n=4, seed=2, K=14)
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ds.reserve(candidates=1 << 16, contacts=1 << 16)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    ds.traverse(sc.pairs)
+    moved = sc.pos.copy()
+    moved[1] += np.float32(0.25)
+    ds.set_poses(sc.quat, moved)  # not refitted: the contacts keep the refit's poses
+    ds.contacts()
+    assert ds.stats().status == 0
+    posed = ds.read_contacts()
+    assert len(posed) > 0
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    world = ds.read_vertices()
+    ds2 = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ds2.set_vertices(world)
+    ds2.refit(kd.REFIT_VERTICES)
+    ds2.traverse_sync(sc.pairs, contacts=True)
+    ref = ds2.read_contacts()
+    def rows(c):
+        return sorted(np.column_stack([c["p"], c["n"], c["depth"][:, None]]).astype(np.float32).view(np.uint32)
+                      .reshape(len(c), -1).tolist())
+    assert rows(posed) == rows(ref)
+    ds.close()
+    ds2.close()
+
+
 def check_against_fp64(oracle, dev_rows, ref64_rows, xa, A, xb, B, pairs):
     """Device FP32 contacts vs the FP64 oracle on the pairs whose discrete
     decisions (overlap, chosen faces, set of generated contact candidates)
