@@ -206,6 +206,12 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
   };
   unsigned max_depth = 0;
   bool failed = false;
+  // Pair index of the deque's entries.  A deque filled from one root pair or
+  // one queue item holds a single pair (entries inherit their parent's pair),
+  // kept in curP; only a claim of several root pairs or frontier entries at
+  // once mixes pairs, and then each entry's pair is kept in sP (warp-uniform).
+  uint32_t curP = 0;
+  bool mixed = false;
 
   unsigned step = 0;
   for (;;) {
@@ -232,6 +238,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         release = 0;
       }
       bool have = false;
+      mixed = false;  // the deque is empty
       if (!init_done) {
         unsigned base = 0;
         if (lane == 0) base = atomicAdd(&ctl->init_head, (unsigned)a.init_chunk);
@@ -240,18 +247,21 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
           int n = (int)min((unsigned)a.init_chunk, n_init - base);
           release += n;
           have = true;
+          uint32_t p0 = 0;
           if (lane < n && a.entries) {
             // a pending node pair of a frontier (its tests are counted already)
             const uint4 e = a.entries[base + lane];
             pushA[0] = e.x;
             pushB[0] = e.y;
             slotP[0] = e.z;
+            p0 = e.z;
             push_mask = 1;
           } else if (lane < n) {
             // root test (kdop_tandem_traversal.h:164), then the traversal's own
             // test of the root pair (:42), both counted as the reference does.
             uint32_t pid = pair_base + base + lane;
             if (a.order) pid = a.order[pid];
+            p0 = pid;
             uint2 mp = a.pairs[pid];
             uint32_t ra = NO_NODE, rb = NO_NODE;
             if (mp.x < a.n_meshes && mp.y < a.n_meshes) {
@@ -278,6 +288,10 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
               }
             }
           }
+          if (n > 1)
+            mixed = true;  // entries of several pairs
+          else
+            curP = __shfl_sync(0xffffffffu, p0, 0);
         } else {
           init_done = true;
         }
@@ -318,8 +332,8 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         if (lane == 0) {
           a.q_tags[claim] = 0u;
           sAB[top & MASK] = make_uint2(it.x, it.y);
-          sP[top & MASK] = it.z;
         }
+        curP = it.z;  // the deque was empty: one pair
         top += 1;
         release += 1;
         claim = 0xFFFFFFFFu;
@@ -340,7 +354,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         if (i < n) {
           const int at = (top + i) & MASK;
           eab[b] = sAB[at];
-          ep[b] = sP[at];
+          ep[b] = mixed ? sP[at] : curP;
         }
         const int64_t ta = (int64_t)((eab[b].x & NODE_MASK) >> 1) * (2 * NW);
         const int64_t tb = (int64_t)((eab[b].y & NODE_MASK) >> 1) * (2 * NW);
@@ -477,7 +491,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
             if (push_mask & (1u << k)) {
               const int at = (top + pbase[k] + __popc(pm[k] & lt_mask)) & MASK;
               sAB[at] = make_uint2(pushA[k], pushB[k]);
-              sP[at] = slotP[k];
+              if (mixed) sP[at] = slotP[k];
             }
           }
           top += tot_p;
@@ -529,7 +543,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
         if (lane < room) {
           int at = (bot + lane) & MASK;
           uint2 ab = sAB[at];
-          a.q_items[t0 + lane] = make_uint4(ab.x, ab.y, sP[at], 0u);
+          a.q_items[t0 + lane] = make_uint4(ab.x, ab.y, mixed ? sP[at] : curP, 0u);
         }
         __threadfence();
         __syncwarp();
