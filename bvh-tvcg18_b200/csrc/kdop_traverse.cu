@@ -177,6 +177,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
   const int CAP = a.stack_cap;
   const int MASK = CAP - 1;
   // this warp's deque: CAP entries of (A, B) words, then CAP pair indices
+  // (written and read only while the deque mixes pairs, see curP below)
   uint32_t* wbase = smem + (size_t)wib * 3 * CAP;
   uint2* sAB = reinterpret_cast<uint2*>(wbase);
   uint32_t* sP = wbase + 2 * CAP;
