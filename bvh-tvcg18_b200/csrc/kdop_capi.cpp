@@ -83,6 +83,7 @@ struct kdop_scene_ext {
   std::vector<uint32_t> pairs_host;  // last traversed mesh pairs
   std::vector<uint32_t> order_host;  // their order of processing
   int64_t graph_kernels = 0;
+  int graph_refit_mode = 0;  // refit mode of the captured step
   kdop_traverse_opts tuned{};
   bool has_tuned = false;
 };
@@ -647,12 +648,23 @@ int kdop_set_motion(kdop_scene* s, const float* lin, const float* ang, float pha
   return KDOP_OK;
 }
 
+// The contact kernels and the adjoint read the posed vertex array after a
+// pose / deform refit.  A mode set by a graph capture whose step has not run
+// yet leaves it unwritten: pose the vertices with the current poses first.
+static cudaError_t ensure_posed(kdop_scene* s) {
+  if (s->refit_mode <= KDOP_REFIT_VERTICES || s->posed_valid) return cudaSuccess;
+  cudaError_t e = kdop::launch_world(s, s->refit_mode, s->posed);
+  if (e == cudaSuccess) s->posed_valid = true;
+  return e;
+}
+
 int kdop_refit(kdop_scene* s, int mode) {
   if (!s) return KDOP_ERR_INVALID;
   if (mode < KDOP_REFIT_VERTICES || mode > KDOP_REFIT_DEFORM) return fail(s->ctx, KDOP_ERR_INVALID, "bad refit mode");
   cudaSetDevice(s->ctx->device);
   s->refit_mode = mode;
   KDOP_CUDA(s->ctx, kdop::launch_refit(s, mode));
+  if (mode != KDOP_REFIT_VERTICES) s->posed_valid = true;
   return KDOP_OK;
 }
 
@@ -662,20 +674,12 @@ int kdop_read_vertices(kdop_scene* s, float* xyz, int64_t cap) {
   if (s->nv == 0) return KDOP_OK;
   std::vector<float4> h((size_t)s->nv);
   float4* src = s->world;
-  float4* tmp = nullptr;
-  int mode = s->refit_mode < 0 ? 0 : s->refit_mode;
-  if (mode != KDOP_REFIT_VERTICES) {
-    KDOP_CUDA(s->ctx, cudaMalloc((void**)&tmp, (size_t)s->nv * sizeof(float4)));
-    cudaError_t e = kdop::launch_world(s, mode, tmp);
-    if (e != cudaSuccess) {
-      cudaFree(tmp);
-      return cuda_fail(s->ctx, e, "launch_world");
-    }
-    src = tmp;
+  if (s->refit_mode > KDOP_REFIT_VERTICES) {
+    KDOP_CUDA(s->ctx, ensure_posed(s));
+    src = s->posed;
   }
   cudaError_t e = cudaMemcpyAsync(h.data(), src, (size_t)s->nv * sizeof(float4), cudaMemcpyDeviceToHost, s->ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->ctx->stream);
-  if (tmp) cudaFree(tmp);
   if (e != cudaSuccess) return cuda_fail(s->ctx, e, "read vertices");
   for (int64_t i = 0; i < s->nv; ++i) {
     xyz[3 * i] = h[i].x;
@@ -1005,6 +1009,7 @@ int kdop_contacts(kdop_scene* s) {
   if (!s) return KDOP_ERR_INVALID;
   if (!s->traversed) return fail(s->ctx, KDOP_ERR_STATE, "kdop_contacts before kdop_traverse");
   cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, ensure_posed(s));
   KDOP_CUDA(s->ctx, kdop::launch_contacts(s));
   s->contacted = true;
   return KDOP_OK;
@@ -1123,6 +1128,7 @@ int kdop_contacts_adjoint(kdop_scene* s, const float* dd, const float* dn, float
   if (!s || !dd || !grad) return KDOP_ERR_INVALID;
   if (!s->contacted) return fail(s->ctx, KDOP_ERR_STATE, "adjoint before kdop_contacts");
   cudaSetDevice(s->ctx->device);
+  KDOP_CUDA(s->ctx, ensure_posed(s));
   if (memory == KDOP_DEVICE) {
     KDOP_CUDA(s->ctx, kdop::launch_adjoint(s, dd, dn, grad));
     return KDOP_OK;
@@ -1171,7 +1177,15 @@ int kdop_graph_capture(kdop_scene* s, int refit_mode, int64_t n_pairs, const uin
   KDOP_CUDA(s->ctx, kdop::traverse_prepare(s->K, kdop::traverse_smem_bytes(p.block_warps, p.stack_cap)));
   KDOP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
   long long before = s->ctx->launches;
-  KDOP_CUDA(s->ctx, cudaStreamBeginCapture(s->ctx->stream, cudaStreamCaptureModeRelaxed));
+  // the captured contact kernels take their vertex source from the refit
+  // mode: the graph's, not the one of the last direct refit
+  const int old_refit_mode = s->refit_mode;
+  s->refit_mode = refit_mode;
+  cudaError_t eb = cudaStreamBeginCapture(s->ctx->stream, cudaStreamCaptureModeRelaxed);
+  if (eb != cudaSuccess) {
+    s->refit_mode = old_refit_mode;
+    return cuda_fail(s->ctx, eb, "cudaStreamBeginCapture");
+  }
   cudaError_t e = cudaSuccess;
   if (flags & 1) e = kdop::launch_motion(s);
   if (e == cudaSuccess) e = kdop::launch_refit(s, refit_mode);
@@ -1182,17 +1196,20 @@ int kdop_graph_capture(kdop_scene* s, int refit_mode, int64_t n_pairs, const uin
   s->ctx->launches = before;
   if (e != cudaSuccess || e2 != cudaSuccess) {
     if (g) cudaGraphDestroy(g);
+    s->refit_mode = old_refit_mode;
     return cuda_fail(s->ctx, e != cudaSuccess ? e : e2, "graph capture");
   }
   s->graph = g;
   e = cudaGraphInstantiate(&s->graph_exec, g, 0);
   if (e != cudaSuccess) {
     kdop_graph_release(s);
+    s->refit_mode = old_refit_mode;
     return cuda_fail(s->ctx, e, "cudaGraphInstantiate");
   }
   size_t n_nodes = 0;
   cudaGraphGetNodes(g, nullptr, &n_nodes);
   ext(s)->graph_kernels = (int64_t)n_nodes;
+  ext(s)->graph_refit_mode = refit_mode;
   s->refit_mode = refit_mode;
   s->traversed = true;
   s->contacted = true;
@@ -1208,6 +1225,7 @@ int kdop_graph_launch(kdop_scene* s) {
   cudaSetDevice(s->ctx->device);
   KDOP_CUDA(s->ctx, cudaGraphLaunch(s->graph_exec, s->ctx->stream));
   s->ctx->launches += ext(s)->graph_kernels;
+  if (ext(s)->graph_refit_mode != KDOP_REFIT_VERTICES) s->posed_valid = true;
   return KDOP_OK;
 }
 

@@ -106,6 +106,7 @@ struct kdop_scene {
   float4* rest = nullptr;
   float4* world = nullptr;
   float4* posed = nullptr;  // world positions a pose / deform refit computes before its leaf pass
+  bool posed_valid = false;  // posed holds the positions of an executed pose / deform refit
   uint4* tets = nullptr;  // global vertex indices
   uint8_t* surf = nullptr;
   float4* nodes = nullptr;

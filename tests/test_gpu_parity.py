@@ -166,6 +166,35 @@ def test_contacts_use_the_positions_of_the_last_refit(ctx):
     ds2.close()
 
 
+def test_pose_graph_before_its_first_launch(ctx, oracle):
+    """A scene whose pose-mode step is captured but not yet launched has no
+    posed vertices from a refit: reading them poses the vertices with the
+    current poses, and the first launch gives the rows of a plain pose refit."""
+    sc = scenes.touching_pair(n=4, seed=3, K=14)
+    ref = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ref.reserve(candidates=1 << 16, contacts=1 << 16)
+    ref.set_poses(sc.quat, sc.pos)
+    ref.refit(kd.REFIT_POSE)
+    ref.traverse_sync(sc.pairs, contacts=True)
+    want = ref.read_contacts()
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ds.reserve(candidates=1 << 16, contacts=1 << 16)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.graph_capture(sc.pairs, refit_mode=kd.REFIT_POSE)
+    xw = np.concatenate([oracle.rotate(sc.quat[i], sc.pos[i], m.xyz) for i, m in enumerate(sc.meshes)])
+    assert ds.read_vertices().tobytes() == np.ascontiguousarray(xw, np.float32).tobytes()
+    ds.graph_launch()
+    assert ds.stats().status == 0
+    got = ds.read_contacts()
+    def rows(c):
+        return sorted(np.column_stack([c["p"], c["n"], c["depth"][:, None]]).astype(np.float32).view(np.uint32)
+                      .reshape(len(c), -1).tolist())
+    assert len(want) > 0 and rows(got) == rows(want)
+    ds.graph_release()
+    ds.close()
+    ref.close()
+
+
 def check_against_fp64(oracle, dev_rows, ref64_rows, xa, A, xb, B, pairs):
     """Device FP32 contacts vs the FP64 oracle on the pairs whose discrete
     decisions (overlap, chosen faces, set of generated contact candidates)
