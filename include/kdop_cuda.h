@@ -147,7 +147,10 @@ typedef enum {
 /* Bottom-up refit of every tree of the scene; the mode also fixes how the
  * contact kernels obtain world positions until the next refit. */
 int kdop_refit(kdop_scene* scene, int mode);
-/* Copies the current world positions (n_verts_total*3) to host memory. */
+/* Copies the world positions (n_verts_total*3) to host memory: the
+ * kdop_set_vertices positions in KDOP_REFIT_VERTICES mode, else the ones the
+ * last pose / deform refit computed (posed with the current poses when the
+ * mode was set by a captured graph that has not run yet). */
 int kdop_read_vertices(kdop_scene* scene, float* xyz, int64_t cap_verts);
 
 /* ---- tandem traversal (replaces tandem_traversal) ------------------------- */
