@@ -1211,6 +1211,8 @@ int kdop_graph_capture(kdop_scene* s, int refit_mode, int64_t n_pairs, const uin
   ext(s)->graph_kernels = (int64_t)n_nodes;
   ext(s)->graph_refit_mode = refit_mode;
   s->refit_mode = refit_mode;
+  // capturing runs nothing: the posed array holds no step of this graph yet
+  s->posed_valid = false;
   s->traversed = true;
   s->contacted = true;
   s->last_pairs = n_pairs;
@@ -1225,7 +1227,10 @@ int kdop_graph_launch(kdop_scene* s) {
   cudaSetDevice(s->ctx->device);
   KDOP_CUDA(s->ctx, cudaGraphLaunch(s->graph_exec, s->ctx->stream));
   s->ctx->launches += ext(s)->graph_kernels;
-  if (ext(s)->graph_refit_mode != KDOP_REFIT_VERTICES) s->posed_valid = true;
+  // the step just enqueued refits in the graph's mode: the contacts, the
+  // adjoint and read-backs follow it, whatever direct refit ran in between
+  s->refit_mode = ext(s)->graph_refit_mode;
+  if (s->refit_mode != KDOP_REFIT_VERTICES) s->posed_valid = true;
   return KDOP_OK;
 }
 

@@ -199,9 +199,6 @@ typedef struct {
   int32_t reserved;
 } kdop_stats;
 
-/* Enqueues the traversal of n_pairs mesh pairs (pairs[2i] = mesh A, pairs[2i+1]
- * = mesh B).  Asynchronous: read results with kdop_get_stats.  opts NULL =
- * defaults. */
 /* Broad phase (replaces broad::find_overlaps, SIMULATION/BROAD/BROAD/include/
  * broad_find_overlaps.h:44-125; its all-pair and grid algorithms report the
  * same set): the mesh pairs (i, j), i < j, whose boxes overlap, sorted
@@ -215,6 +212,9 @@ typedef struct {
 int kdop_broad_phase(kdop_scene* scene, const float* positions, int memory, uint32_t* out_pairs, int64_t cap,
                      int64_t* n_pairs);
 
+/* Enqueues the traversal of n_pairs mesh pairs (pairs[2i] = mesh A, pairs[2i+1]
+ * = mesh B).  Asynchronous: read results with kdop_get_stats.  opts NULL =
+ * defaults. */
 int kdop_traverse(kdop_scene* scene, int64_t n_pairs, const uint32_t* pairs, int memory,
                   const kdop_traverse_opts* opts);
 

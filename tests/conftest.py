@@ -17,6 +17,9 @@ for p in (ROOT, PKG):
         sys.path.insert(0, p)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden", "reference_golden.npz")
+GOLDEN_LARGE = os.path.join(ROOT, "tests", "golden", "reference_large.json")
+sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+from make_golden_large import canonical_candidates, canonical_contacts, digest  # noqa: E402,F401
 
 
 def pytest_configure(config):
@@ -47,6 +50,14 @@ def reference():
 @pytest.fixture(scope="session")
 def golden():
     return np.load(GOLDEN)
+
+
+@pytest.fixture(scope="session")
+def golden_large():
+    """Digests of the reference's own results on the full-size workloads."""
+    import json
+    with open(GOLDEN_LARGE) as f:
+        return json.load(f)
 
 
 @pytest.fixture(scope="session")

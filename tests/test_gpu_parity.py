@@ -195,6 +195,88 @@ def test_pose_graph_before_its_first_launch(ctx, oracle):
     ref.close()
 
 
+def test_pose_graph_capture_after_an_earlier_pose_refit(ctx, oracle):
+    """A direct pose refit, then a pose change, then the capture of a pose
+    step: before the first launch the vertices read back are posed with the
+    current poses (not the earlier refit's), and the first launch gives the
+    rows of a plain pose refit at those poses."""
+    sc = scenes.touching_pair(n=4, seed=6, K=14)
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ds.reserve(candidates=1 << 16, contacts=1 << 16)
+    old = sc.pos.copy()
+    old[1] += np.float32(0.3)
+    ds.set_poses(sc.quat, old)
+    ds.refit(kd.REFIT_POSE)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.graph_capture(sc.pairs, refit_mode=kd.REFIT_POSE)
+    xw = np.concatenate([oracle.rotate(sc.quat[i], sc.pos[i], m.xyz) for i, m in enumerate(sc.meshes)])
+    assert ds.read_vertices().tobytes() == np.ascontiguousarray(xw, np.float32).tobytes()
+    ds.graph_launch()
+    assert ds.stats().status == 0
+    ref = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ref.reserve(candidates=1 << 16, contacts=1 << 16)
+    ref.set_poses(sc.quat, sc.pos)
+    ref.refit(kd.REFIT_POSE)
+    ref.traverse_sync(sc.pairs, contacts=True)
+    assert len(ref.read_contacts()) > 0
+    assert contact_rows(ds.read_contacts()) == contact_rows(ref.read_contacts())
+    ds.graph_release()
+    ds.close()
+    ref.close()
+
+
+def test_graph_launch_restores_the_graph_refit_mode(ctx):
+    """Capture a pose step, refit other positions directly in vertex mode, then
+    launch the graph: the contacts, the vertices read back and the adjoint all
+    follow the graph's pose step, as after a plain pose refit."""
+    import torch
+    sc = scenes.touching_pair(n=4, seed=7, K=14)
+    ref = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ref.reserve(candidates=1 << 16, contacts=1 << 16)
+    ref.set_poses(sc.quat, sc.pos)
+    ref.refit(kd.REFIT_POSE)
+    ref.traverse_sync(sc.pairs, contacts=True)
+    want = ref.read_contacts()
+    assert len(want) > 0
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ds.reserve(candidates=1 << 16, contacts=1 << 16)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.graph_capture(sc.pairs, refit_mode=kd.REFIT_POSE)
+    other = np.concatenate([m.xyz for m in sc.meshes]) + np.float32(0.05)
+    ds.set_vertices(other)
+    ds.refit(kd.REFIT_VERTICES)
+    ds.graph_launch()
+    assert ds.stats().status == 0
+    got = ds.read_contacts()
+    assert contact_rows(got) == contact_rows(want)
+    assert ds.read_vertices().tobytes() == ref.read_vertices().tobytes()
+
+    def grad(scene, rows):
+        n = len(rows)
+        dd = torch.tensor(2.0 * rows["depth"], device="cuda")
+        dn = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+        g = torch.zeros((int(scene.v_off[-1]), 3), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        scene.adjoint(dd, dn, g)
+        scene.ctx.synchronize()
+        return g.cpu().numpy().astype(np.float64)
+
+    # same rows in the same order (one traversal state each): the gradients
+    # differ only by the arrival order of float atomics
+    gr, gd = grad(ref, want), grad(ds, got)
+    scale = max(np.abs(gr).max(), 1e-30)
+    assert np.abs(gr).max() > 0
+    assert np.abs(gd - gr).max() <= 1e-5 * scale
+    ds.graph_release()
+    ds.close()
+    ref.close()
+
+
+def contact_rows(c):
+    return sorted(np.column_stack([c["p"], c["n"], c["depth"][:, None]]).astype(np.float32).view(np.uint32)
+                  .reshape(len(c), -1).tolist())
+
+
 def check_against_fp64(oracle, dev_rows, ref64_rows, xa, A, xb, B, pairs):
     """Device FP32 contacts vs the FP64 oracle on the pairs whose discrete
     decisions (overlap, chosen faces, set of generated contact candidates)

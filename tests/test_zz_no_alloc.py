@@ -83,3 +83,52 @@ def test_noalloc_rejects_oversized_requests(ctx):
     assert lib.kdop_traverse_noalloc(ds.h, 1 << 31, buf.data_ptr(), buf.data_ptr(), 8, buf.data_ptr(), None) == \
         kd.lib.ERR_CAPACITY
     assert lib.kdop_traverse_noalloc(ds.h, 1, None, buf.data_ptr(), 8, buf.data_ptr(), None) == kd.lib.ERR_INVALID
+
+
+def test_noalloc_queue_exhaustion_is_reported_and_the_next_call_is_clean(ctx):
+    """A run that needs more than the static array's 65,536 queue entries sets
+    error bit 2 (queue full) in counters[3] and still returns: entries that
+    found no room are dropped and never counted as outstanding work, so the
+    waiting warps see the work count reach zero.  The next call clears the
+    array and gives the allocating entry point's result again."""
+    import torch
+
+    sc = scenes.config3(n_pairs=24, seed=5, min_tets=2e4, max_tets=6e4)
+    ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
+    ds.set_poses(sc.quat, sc.pos)
+    ds.refit(kd.REFIT_POSE)
+    # smallest deques and eager donation: most node pairs pass through the queue
+    hungry = ds.opts(stack_cap=64, donate_min=1, init_chunk=1)
+    st = ds.traverse_sync(sc.pairs, hungry)
+    assert st.queue_used > 65536, f"case too small to exhaust the static queue ({st.queue_used} entries)"
+    base = ds.traverse_sync(sc.pairs)
+    want = sorted_rows(ds.candidates().astype(np.int64))
+
+    lib = ds.lib
+    lib.kdop_traverse_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+    lib.kdop_traverse_noalloc.restype = ctypes.c_int
+    n = len(sc.pairs)
+    cap = int(base.n_candidates) + 64
+    pairs_d = torch.tensor(sc.pairs.astype(np.int32), device="cuda")
+    cand_d = torch.empty(3 * cap, dtype=torch.int32, device="cuda")
+    cnt_d = torch.empty(4, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    rc = lib.kdop_traverse_noalloc(ds.h, n, pairs_d.data_ptr(), cand_d.data_ptr(), cap, cnt_d.data_ptr(),
+                                   ctypes.byref(hungry))
+    assert rc == 0, rc
+    ctx.synchronize()
+    counts = cnt_d.cpu().numpy()
+    assert counts[3] & 2, f"queue exhaustion not reported (error bits {counts[3]})"
+    assert not counts[3] & 1, "the run gave up waiting instead of ending"
+
+    rc = lib.kdop_traverse_noalloc(ds.h, n, pairs_d.data_ptr(), cand_d.data_ptr(), cap, cnt_d.data_ptr(), None)
+    assert rc == 0, rc
+    ctx.synchronize()
+    counts = cnt_d.cpu().numpy()
+    assert counts[3] == 0, f"error bits {counts[3]} after the exhausted run"
+    assert counts[0] == base.n_candidates and counts[1] == base.n_tests
+    c = cand_d.cpu().numpy().view(np.uint32).astype(np.int64)
+    k = int(counts[0])
+    got = _global_to_local(c[:k], c[cap:cap + k], c[2 * cap:2 * cap + k], sc.pairs.astype(np.int64), ds.t_off)
+    assert np.array_equal(sorted_rows(got), want)
