@@ -20,7 +20,6 @@ import argparse
 import json
 import math
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -103,6 +102,17 @@ class Dist:
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
+    def gather(self, values) -> list:
+        """Every rank's list of numbers, in rank order (all-gather)."""
+        if not self.pg:
+            return [list(values)]
+        import torch
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=dev)
+        parts = [torch.empty_like(t) for _ in range(self.world)]
+        self.pg.all_gather(parts, t)
+        return [p.cpu().tolist() for p in parts]
+
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
@@ -175,31 +185,53 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-# node-pair tests of one full config-3 traversal (512 pairs), the launch the
-# committed traversal capture is scaled to
-CONFIG3_FULL_TESTS = 1807762098
+def shape_key(opts) -> str:
+    """The traversal launch shape (every autotuned knob) as one string."""
+    o = opts.as_dict()
+    return ",".join(f"{k}={o[k]}" for k in ("block_warps", "stack_cap", "init_chunk", "donate_min", "load_group",
+                                            "wave_pairs", "smem_carveout"))
 
 
-def ncu_traffic(name: str):
-    """dram bytes per launch from a committed ncu summary (profiles/<name>.md)."""
-    path = os.path.join(ROOT, "profiles", name)
+def traverse_dram_capture(workload: str, opts):
+    """DRAM bytes per node-pair test and L1 data-pipe use of the traversal
+    launch, from the ncu capture of the same launch shape on the same
+    workload family (profiles/traverse_dram.json); None when no capture of
+    this shape exists, so that no traffic is quoted for a shape nobody
+    measured."""
+    path = os.path.join(ROOT, "profiles", "traverse_dram.json")
     if not os.path.exists(path):
         return None
-    m = re.search(r"dram_bytes_per_full_launch\s*=\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
+    with open(path) as f:
+        d = json.load(f)
+    return d.get("captures", {}).get(workload, {}).get(shape_key(opts))
 
 
-def workload(args, rank: int):
-    from kdop_b200 import scenes
+def workload(args, rank: int = 0, world: int = 1):
+    """This rank's share of the workload.  The batched configurations are one
+    workload of `pairs` per GPU x world pairs, split over the ranks by
+    estimated cost (kdop_b200.sharding.partition: largest pair first onto the
+    least-loaded rank), so every GPU holds about one headline batch (weak
+    scaling).  The single-pair configurations run as replicas."""
+    from kdop_b200 import scenes, sharding
     if args.workload == "config2":
         return scenes.config2()
-    if args.workload == "config5":
-        return scenes.config5(n_pairs=args.pairs or 256)
-    if args.workload == "config4":
-        return scenes.config4(n_pairs=args.pairs or 64)
     if args.workload == "config1":
         return scenes.config1()
-    return scenes.config3(n_pairs=args.pairs or 512, seed=2 + rank)
+    if args.workload == "config3":
+        total = (args.pairs or 512) * world
+        # sizes of every pair first (no mesh built), then only this rank's meshes
+        sizes = scenes.config3(n_pairs=total, keep=[]).extra["pair_tets"]
+        pairs = np.arange(2 * total, dtype=np.uint32).reshape(-1, 2)
+        mine = sharding.partition(pairs, np.repeat(sizes // 2, 2), world)[rank]
+        sc = scenes.config3(n_pairs=total, keep=mine)
+    else:
+        full = (scenes.config5(n_pairs=(args.pairs or 256) * world) if args.workload == "config5" else
+                scenes.config4(n_pairs=(args.pairs or 64) * world))
+        mine = sharding.partition(full.pairs, [m.n_tets for m in full.meshes], world)[rank]
+        sc = scenes.subset(full, mine)
+    sc.extra["pairs_total"] = int(len(sc.extra["pair_tets"]) if "pair_tets" in sc.extra else
+                                  (args.pairs or (256 if args.workload == "config5" else 64)) * world)
+    return sc
 
 
 def cpu_sample(sc, tests_per_pair, budget_tests):
@@ -233,6 +265,25 @@ def reference_time(sc, n_pairs, threads, repeats=1):
     return sec, contacts
 
 
+def reference_workload(args, world: int):
+    """The first pairs of the CUDA arm's whole workload (all of it at one GPU),
+    enough for the reference arm's bounded sample."""
+    from kdop_b200 import scenes
+    if args.workload == "config3":
+        total = (args.pairs or 512) * world
+        sc = scenes.config3(n_pairs=total, keep=range(min(total, args.pairs or 512)))
+    elif args.workload in ("config4", "config5"):
+        per = args.pairs or (256 if args.workload == "config5" else 64)
+        full = (scenes.config5(n_pairs=per * world) if args.workload == "config5" else
+                scenes.config4(n_pairs=per * world))
+        sc = scenes.subset(full, range(per))
+        total = per * world
+    else:
+        return workload(args)
+    sc.extra["pairs_total"] = total
+    return sc
+
+
 # ---- reference arm ----------------------------------------------------------------
 def run_reference(args):
     dist = Dist("gloo")
@@ -244,22 +295,25 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU path not built (oracle/_ref missing)"}))
         return
     threads = os.cpu_count() or 1
-    sc = workload(args, 0)
-    tpp = oracle_tests_per_pair(sc)
-    # per step: a bounded sample of the workload, sized so that the whole run
-    # takes about 90 s on all threads (at most 4 s a step)
-    per_step_s = min(4.0, 90.0 / max(args.steps + args.warmup, 1))
+    sc = reference_workload(args, dist.world)
+    tpp = oracle_tests_per_pair(sc, threads=threads)
+    # per step: the workload's first pairs, all of them when they fit, sized
+    # so that the whole run takes at most about 3 minutes on all threads (at
+    # most 8 s a step)
+    per_step_s = min(8.0, 180.0 / max(args.steps + args.warmup, 1))
     n, tests = cpu_sample(sc, tpp, budget_tests=per_step_s * 30e6 * threads)
     reps = args.warmup + max(args.steps, 1)
     secs, _ = reference_time(sc, n, threads, repeats=reps)
     times = (secs if isinstance(secs, list) else [secs])[args.warmup:]
     t = sum(times) / len(times)
     value = tests / t
-    sample = f"first {n} of {len(sc.pairs)} pairs per step ({tests} node-pair tests)"
+    total = int(sc.extra.get("pairs_total", len(sc.pairs)))
+    sample = (f"all {n} pairs per step" if n == total else f"first {n} of {total} pairs per step") + \
+        f" ({tests} node-pair tests), one-chunk trees, pose + refit + tandem traversal with contacts"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": sc.name, "pairs": int(len(sc.pairs)), "K": sc.K,
+            "config": {"workload": sc.name, "pairs": total, "K": sc.K,
                        "sample_pairs": n, "threads": threads},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
                              "sample": sample},
@@ -382,7 +436,7 @@ def run_cuda(args):
 
     dist = Dist("nccl")
     torch.cuda.set_device(dist.local)
-    sc = workload(args, dist.rank)
+    sc = workload(args, dist.rank, dist.world)
     ctx = kd.Context(dist.local)
     stream = torch.cuda.ExternalStream(ctx.stream)
     ds = kd.DeviceScene(ctx, sc.K, sc.meshes)
@@ -453,6 +507,7 @@ def run_cuda(args):
     ms_max = dist.max(ms)
     total_tests = dist.sum(float(tests_per_step))
     value = total_tests / (ms_max * 1e-3)
+    per_rank = dist.gather([len(sc.pairs), sc.n_tets, tests_per_step, ms])
 
     # dominant kernel: the batched traversal launch, timed alone
     reps = 5
@@ -470,11 +525,11 @@ def run_cuda(args):
     alg_bytes = state_tests * 2 * node_bytes
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (trav_ms * 1e-3) / 1e9
-    # the committed capture covers the full 512-pair config-3 launch; DRAM
-    # bytes grow with the traversal work, so other pair counts scale by tests
-    traffic = ncu_traffic("traverse_config3.md") if args.workload == "config3" else None
-    if traffic is not None and len(sc.pairs) != 512:
-        traffic = traffic * state_tests / CONFIG3_FULL_TESTS
+    # DRAM bytes of this launch: the capture of the same launch shape on a
+    # smaller case of the same generator, scaled by node-pair tests (the
+    # launch's DRAM traffic grows with its tests)
+    cap = traverse_dram_capture(args.workload, opts)
+    traffic = cap["dram_bytes_per_test"] * state_tests if cap else None
 
     # plain: one traversal launch per mesh pair, same trees and descent rule;
     # the faster of the default and the batched-tuned launch shape
@@ -576,22 +631,38 @@ def run_cuda(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": sc.name, "pairs_per_gpu": int(len(sc.pairs)), "tets_per_gpu": int(sc.n_tets),
-                       "K": sc.K, "node_bytes": node_bytes, "parallelism": f"pairs sharded, {dist.world} rank(s)",
+            "config": {"workload": sc.name, "pairs_per_gpu": [int(r[0]) for r in per_rank],
+                       "tets_per_gpu": [int(r[1]) for r in per_rank],
+                       "pairs_total": int(sc.extra.get("pairs_total", len(sc.pairs))),
+                       "K": sc.K, "node_bytes": node_bytes,
+                       "parallelism": (f"{sc.extra.get('pairs_total', len(sc.pairs))} pairs partitioned by cost over "
+                                       f"{dist.world} rank(s) (kdop_b200.sharding.partition), no collective on "
+                                       f"the data path" if "pair_ids" in sc.extra else
+                                       f"one pair, {dist.world} replica(s)"),
+                       "tests_per_gpu": [int(r[2]) for r in per_rank],
+                       "ms_per_step_per_gpu": [r[3] for r in per_rank],
                        "l2": (f"inputs larger than L2 (node records {info['n_nodes'] * node_bytes / 1e9:.2f} GB)"
                               if info['n_nodes'] * node_bytes > 126e6 else
                               f"inputs fit in L2 (node records {info['n_nodes'] * node_bytes / 1e6:.1f} MB), no flush"),
                        "step": "CUDA graph: pose transform + refit, batched traversal, contacts",
-                       "tests_per_step_per_gpu": int(tests_per_step), "candidates": int(st2.n_candidates),
+                       "candidates": int(st2.n_candidates),
                        "contacts": int(st2.n_contacts), "traverse_opts": opts.as_dict(), "autotuned": tuned},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "traverse_kernel (batched, one persistent launch)",
-                         "launch_ms": trav_ms, "algorithmic_bytes_per_launch": alg_bytes,
-                         # DRAM bytes the launch really moves (ncu) over its live duration: the
-                         # algorithmic bytes are mostly served by L1/L2 (records reused per test)
+                         "launch_ms": trav_ms, "launch_shape": shape_key(opts),
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         # three readings side by side: `frac` counts every test's two node
+                         # records (most are served by L1/L2: a cache-reuse figure, not HBM);
+                         # dram_frac is the DRAM bytes this launch shape really moves (ncu)
+                         # over the live launch time; l1_lsu_pct is the busiest unit, the L1
+                         # data pipe, as a % of its peak in the same capture
+                         "frac_kind": "algorithmic bytes (2 node records per test) / launch time / HBM peak",
                          "dram_gbs": (traffic / (trav_ms * 1e-3) / 1e9) if traffic else None,
-                         "dram_frac": (traffic / (trav_ms * 1e-3) / 1e9 / peak) if traffic else None},
+                         "dram_frac": (traffic / (trav_ms * 1e-3) / 1e9 / peak) if traffic else None,
+                         "l1_lsu_pct": cap["l1_lsu_pct"] if cap else None,
+                         "traffic_source": (cap["source"] if cap else
+                                            "no ncu capture of this launch shape: traffic not quoted")},
             "plain": plain,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),

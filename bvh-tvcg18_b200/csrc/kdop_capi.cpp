@@ -718,6 +718,13 @@ int kdop_resolve_traverse_opts(const kdop_scene* s, const kdop_traverse_opts* o,
   return KDOP_OK;
 }
 
+// Size class of a scene for the autotuner's cache: floor(log2(tets of all
+// its meshes)).
+static int tune_size_class(const kdop_scene* s) {
+  const int64_t tets = s->t_off.empty() ? 0 : s->t_off.back();
+  return tets > 0 ? (int)std::log2((double)tets) : 0;
+}
+
 extern "C" {
 
 int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
@@ -734,15 +741,24 @@ int kdop_traverse_opts_default(const kdop_scene* s, kdop_traverse_opts* o) {
   o->wave_pairs = 0;
   o->smem_carveout = 0;
   if (s) {
+    // this scene's own autotuned choice, else one cached on the context for
+    // the same K and size class
     kdop_scene_ext* x = ext(const_cast<kdop_scene*>(s));
+    const kdop_traverse_opts* t = nullptr;
     if (x->has_tuned) {
-      o->block_warps = x->tuned.block_warps;
-      o->stack_cap = x->tuned.stack_cap;
-      o->init_chunk = x->tuned.init_chunk;
-      o->donate_min = x->tuned.donate_min;
-      o->load_group = x->tuned.load_group;
-      o->wave_pairs = x->tuned.wave_pairs;
-      o->smem_carveout = x->tuned.smem_carveout;
+      t = &x->tuned;
+    } else {
+      auto it = s->ctx->tuned.find(std::make_pair(s->K, tune_size_class(s)));
+      if (it != s->ctx->tuned.end()) t = &it->second;
+    }
+    if (t) {
+      o->block_warps = t->block_warps;
+      o->stack_cap = t->stack_cap;
+      o->init_chunk = t->init_chunk;
+      o->donate_min = t->donate_min;
+      o->load_group = t->load_group;
+      o->wave_pairs = t->wave_pairs;
+      o->smem_carveout = t->smem_carveout;
     }
   }
   return KDOP_OK;
@@ -1235,10 +1251,11 @@ int kdop_graph_launch(kdop_scene* s) {
 }
 
 // Times one traversal configuration: a checked warm-up run (growing the
-// buffers if needed), then `repeats` timed runs; returns milliseconds per run
-// or a negative value when the configuration cannot run.
-static float time_config(kdop_scene* s, int64_t n_pairs, const kdop::TravParams& p, int repeats, cudaEvent_t e0,
-                         cudaEvent_t e1) {
+// buffers if needed), then `repeats` runs timed one by one; returns the
+// median milliseconds per run, or a negative value when the configuration
+// cannot run.
+static float time_config(kdop_scene* s, int64_t n_pairs, const kdop::TravParams& p, int repeats,
+                         std::vector<cudaEvent_t>& ev) {
   if (kdop::traverse_smem_bytes(p.block_warps, p.stack_cap) > s->ctx->smem_optin) return -1.f;
   if (kdop::launch_traverse(s, n_pairs, s->pairs, p, 0) != cudaSuccess) return -1.f;
   kdop_stats st;
@@ -1251,33 +1268,46 @@ static float time_config(kdop_scene* s, int64_t n_pairs, const kdop::TravParams&
     r = kdop_get_stats(s, &st);
   }
   if (r != KDOP_OK) return -1.f;
-  cudaEventRecord(e0, s->ctx->stream);
-  for (int k = 0; k < repeats; ++k) kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
-  cudaEventRecord(e1, s->ctx->stream);
-  if (cudaEventSynchronize(e1) != cudaSuccess) return -1.f;
-  float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventRecord(ev[0], s->ctx->stream);
+  for (int k = 0; k < repeats; ++k) {
+    kdop::launch_traverse(s, n_pairs, s->pairs, p, 0);
+    cudaEventRecord(ev[k + 1], s->ctx->stream);
+  }
+  if (cudaEventSynchronize(ev[repeats]) != cudaSuccess) return -1.f;
+  std::vector<float> ms((size_t)repeats);
+  for (int k = 0; k < repeats; ++k) cudaEventElapsedTime(&ms[(size_t)k], ev[k], ev[k + 1]);
   if (kdop_get_stats(s, &st) != KDOP_OK) return -1.f;
-  return ms / (float)repeats;
+  std::nth_element(ms.begin(), ms.begin() + repeats / 2, ms.end());
+  return ms[(size_t)repeats / 2];
 }
 
 int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int memory, int repeats,
                   kdop_traverse_opts* best) {
   if (!s || n_pairs < 0 || (n_pairs > 0 && !pairs)) return KDOP_ERR_INVALID;
   cudaSetDevice(s->ctx->device);
-  if (repeats < 1) repeats = 1;
+  // at least five timed runs per configuration, odd so the median is a run
+  repeats = std::max(repeats, 5) | 1;
   int rc = upload_pairs(s, n_pairs, pairs, memory);
   if (rc != KDOP_OK) return rc;
-  cudaEvent_t e0, e1;
-  KDOP_CUDA(s->ctx, cudaEventCreate(&e0));
-  KDOP_CUDA(s->ctx, cudaEventCreate(&e1));
-  // coordinate descent from the defaults, two sweeps over the knobs
+  std::vector<cudaEvent_t> ev((size_t)repeats + 1, nullptr);
+  for (auto& e : ev) {
+    cudaError_t ce = cudaEventCreate(&e);
+    if (ce != cudaSuccess) {
+      for (auto& f : ev)
+        if (f) cudaEventDestroy(f);
+      return cuda_fail(s->ctx, ce, "cudaEventCreate");
+    }
+  }
+  // Coordinate descent from the defaults, two sweeps over the knobs.  A
+  // challenger replaces the incumbent only when its median is more than 2 %
+  // faster, so that run-to-run noise does not flip the choice.
+  const float kGain = 0.98f;
   kdop_traverse_opts d;
   kdop_traverse_opts_default(nullptr, &d);
   kdop::TravParams cur;
   int mode = 0;
   kdop_resolve_traverse_opts(s, &d, cur, mode);
-  float best_ms = time_config(s, n_pairs, cur, repeats, e0, e1);
+  float best_ms = time_config(s, n_pairs, cur, repeats, ev);
   if (best_ms < 0.f) best_ms = 1e30f;
   const std::vector<int> warps = {4, 8, 16}, caps = {128, 256, 512, 1024}, groups = {1, 2, 4, 8},
                          donate = {32, 64, 128, 256}, waves = {0, 16, 64, 128}, carve = {0, 25, 50, 100},
@@ -1293,16 +1323,15 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
                : &p.init_chunk;
         if (*f == v) continue;
         *f = v;
-        float ms = time_config(s, n_pairs, p, repeats, e0, e1);
-        if (ms >= 0.f && ms < best_ms) {
+        float ms = time_config(s, n_pairs, p, repeats, ev);
+        if (ms >= 0.f && ms < kGain * best_ms) {
           best_ms = ms;
           cur = p;
         }
       }
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  for (auto& e : ev) cudaEventDestroy(e);
   if (best_ms >= 1e30f) return fail(s->ctx, KDOP_ERR_CUDA, "autotune: no configuration ran");
   kdop_traverse_opts bo = d;
   bo.block_warps = cur.block_warps;
@@ -1315,13 +1344,7 @@ int kdop_autotune(kdop_scene* s, int64_t n_pairs, const uint32_t* pairs, int mem
   kdop_scene_ext* x = ext(s);
   x->tuned = bo;
   x->has_tuned = true;
-  int64_t tets = 0;
-  for (int64_t i = 0; i < n_pairs; ++i) {
-    uint32_t a = x->pairs_host[2 * i], b = x->pairs_host[2 * i + 1];
-    tets += (s->t_off[a + 1] - s->t_off[a]) + (s->t_off[b + 1] - s->t_off[b]);
-  }
-  int size_class = tets > 0 ? (int)std::log2((double)tets) : 0;
-  s->ctx->tuned[std::make_pair(s->K, size_class)] = bo;
+  s->ctx->tuned[std::make_pair(s->K, tune_size_class(s))] = bo;
   if (best) *best = bo;
   return KDOP_OK;
 }

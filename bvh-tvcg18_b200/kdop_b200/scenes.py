@@ -112,6 +112,13 @@ def lattice(n: int, jitter: float = 0.0, rng: Optional[np.random.Generator] = No
     return Mesh(xyz.astype(np.float32), tets, surf)
 
 
+def skip_lattice(n: int, jitter: float, rng: np.random.Generator) -> None:
+    """Advances rng past the draws lattice(n, jitter, rng) would take (one
+    64-bit output per uniform double) without building the mesh."""
+    if jitter:
+        rng.bit_generator.advance(3 * (n + 1) ** 3)
+
+
 def surface_map(tets: np.ndarray) -> np.ndarray:
     """Boundary faces by face counting (mesh_array_compute_surface_map.h:41-76):
     the face opposite local vertex v of a tet is on the boundary when no other
@@ -221,25 +228,67 @@ def _pair_poses(rng, n: int, q, p, ia: int, ib: int):
 
 
 def config3(n_pairs: int = 512, seed: int = 2, min_tets: float = 1e3, max_tets: float = 2e5,
-            jitter: float = 0.15, K: int = 14) -> Scene:
+            jitter: float = 0.15, K: int = 14, keep=None) -> Scene:
     """n_pairs mesh pairs; per pair a tet count T drawn log-uniformly from
     [1e3, 2e5] and both meshes n^3 cells with n = round((T/6)^(1/3)); vertex
-    jitter +-0.15; random rotations, centroids U(0,1) mesh radii apart; k = 14."""
+    jitter +-0.15; random rotations, centroids U(0,1) mesh radii apart; k = 14.
+
+    keep (optional): the pair indices to build.  The random stream is the
+    same as for the whole scene (the jitter of the other pairs' meshes is
+    skipped, not drawn), so the kept pairs equal those of config3(n_pairs,
+    seed); the returned scene holds only them, renumbered in the given order,
+    with extra['pair_ids'] the global indices and extra['pair_tets'] the tet
+    count of both meshes of every pair of the whole scene."""
     rng = np.random.default_rng(seed)
-    meshes: List[Mesh] = []
+    keep_set = None if keep is None else set(int(k) for k in keep)
+    built = {}
+    pair_tets = np.zeros(n_pairs, np.int64)
     q, p = _identity(2 * n_pairs)
-    pairs = np.zeros((n_pairs, 2), dtype=np.uint32)
     cache = {}
     for i in range(n_pairs):
         T = math.exp(rng.uniform(math.log(min_tets), math.log(max_tets)))
         n = max(1, int(round((T / 6.0) ** (1.0 / 3.0))))
-        for _ in range(2):
-            meshes.append(lattice(n, jitter, rng))
+        if keep_set is None or i in keep_set:
+            built[i] = [lattice(n, jitter, rng) for _ in range(2)]
+        else:
+            for _ in range(2):
+                skip_lattice(n, jitter, rng)
         _pair_poses(rng, n, q, p, 2 * i, 2 * i + 1)
-        pairs[i] = (2 * i, 2 * i + 1)
+        pair_tets[i] = 2 * 6 * n ** 3
         cache[n] = cache.get(n, 0) + 1
-    return Scene(f"config3: {n_pairs} pairs, 1k-200k tets log-uniform, k={K}", K, meshes, q, p, pairs,
-                 {"sizes": cache})
+    ids = list(range(n_pairs)) if keep is None else [int(k) for k in keep]
+    meshes: List[Mesh] = []
+    sel = []
+    for i in ids:
+        meshes += built[i]
+        sel += [2 * i, 2 * i + 1]
+    pairs = np.arange(2 * len(ids), dtype=np.uint32).reshape(-1, 2)
+    sel = np.array(sel, np.int64)
+    return Scene(f"config3: {n_pairs} pairs, 1k-200k tets log-uniform, k={K}", K, meshes, q[sel].copy(),
+                 p[sel].copy(), pairs, {"sizes": cache, "pair_ids": np.array(ids, np.int64),
+                                        "pair_tets": pair_tets})
+
+
+def subset(sc: Scene, pair_ids) -> Scene:
+    """The pairs pair_ids of a scene (and their meshes), renumbered in order."""
+    ids = [int(i) for i in pair_ids]
+    used: List[int] = []
+    index = {}
+    pairs = np.zeros((len(ids), 2), np.uint32)
+    for k, i in enumerate(ids):
+        for s in range(2):
+            m = int(sc.pairs[i, s])
+            if m not in index:
+                index[m] = len(used)
+                used.append(m)
+            pairs[k, s] = index[m]
+    extra = dict(sc.extra)
+    for key in ("lin_vel", "ang_vel"):
+        if key in extra:
+            extra[key] = np.asarray(extra[key])[used].copy()
+    extra["pair_ids"] = np.array(ids, np.int64)
+    return Scene(sc.name, sc.K, [sc.meshes[m] for m in used], sc.quat[used].copy(), sc.pos[used].copy(), pairs,
+                 extra)
 
 
 def config4(n_pairs: int = 64, n: int = 40, seed: int = 3, K: int = 18) -> Scene:

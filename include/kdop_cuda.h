@@ -180,7 +180,10 @@ typedef struct {
                               KDOP_ERR_TIMEOUT (exercises the bounded waits without a GPU fault) */
 } kdop_traverse_opts;
 
-/* Fills opts with the defaults (or the autotuned choice cached for this scene). */
+/* Fills opts with the defaults, or with the autotuned choice: the scene's own
+ * (kdop_autotune on this scene), else one cached on the scene's context by
+ * kdop_autotune on another scene of the same K and size class (floor(log2)
+ * of the scene's total tet count). */
 int kdop_traverse_opts_default(const kdop_scene* scene, kdop_traverse_opts* opts);
 
 typedef struct {
@@ -347,9 +350,15 @@ int kdop_graph_launch(kdop_scene* scene);
 int kdop_graph_release(kdop_scene* scene);
 
 /* ---- autotuner --------------------------------------------------------------- */
-/* Times traversal configurations (block warps, stack capacity, root chunk,
- * donation threshold) on the given pairs and caches the fastest for this
- * scene's device, K and size class; best (optional) receives it. */
+/* Times traversal configurations on the given pairs -- coordinate descent,
+ * two sweeps, over block warps {4,8,16}, stack capacity {128..1024}, load
+ * group {1,2,4,8}, donation threshold {32..256}, wave pairs {0,16,64,128},
+ * shared-memory carveout {0,25,50,100} and root chunk {1,4}, starting from
+ * the defaults -- and caches the fastest for this scene and, on the scene's
+ * context, for its K and size class (see kdop_traverse_opts_default).  Each
+ * configuration is the median of max(repeats, 5) (rounded up to odd) runs
+ * timed one by one; a challenger replaces the incumbent only when more than
+ * 2 % faster.  best (optional) receives the choice.  Synchronises. */
 int kdop_autotune(kdop_scene* scene, int64_t n_pairs, const uint32_t* pairs, int memory, int repeats,
                   kdop_traverse_opts* best);
 

@@ -7,7 +7,10 @@
 //
 // Built by `make -C oracle adapter` against the reference's headers and
 // libkdop_cuda.so; run by tests/test_gpu_adapter.py on a GPU.
+#include <chrono>
+#include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 #include <algorithm>
@@ -97,54 +100,126 @@ struct Rows : public geometry::ContactsCallback<V> {
   }
 };
 
+// Bitwise comparison of every defined node volume of every chunk level and of
+// the root kDOP.
 template <size_t K>
-static int run(kdop_ctx* ctx, int n, float pen, float angle) {
+static int volume_mismatches(kdop::Tree<T, K> const& a, kdop::Tree<T, K> const& b) {
+  int bad = 0;
+  if (a.number_of_levels() != b.number_of_levels()) return 1 << 20;
+  for (size_t h = 0; h < a.number_of_levels(); ++h) {
+    std::vector<kdop::SubTree<T, K> > const& la = a.super_chunks(h);
+    std::vector<kdop::SubTree<T, K> > const& lb = b.super_chunks(h);
+    if (la.size() != lb.size()) return 1 << 20;
+    for (size_t c = 0; c < la.size(); ++c)
+      for (size_t i = 0; i < la[c].m_nodes.size(); ++i) {
+        if (la[c].m_nodes[i].is_undefined()) continue;
+        for (size_t k = 0; k < K / 2; ++k)
+          if (std::memcmp(&la[c].m_nodes[i].m_volume(k), &lb[c].m_nodes[i].m_volume(k), sizeof(geometry::Interval<T>)))
+            ++bad;
+      }
+  }
+  for (size_t k = 0; k < K / 2; ++k)
+    if (std::memcmp(&a.m_root(k), &b.m_root(k), sizeof(geometry::Interval<T>))) ++bad;
+  return bad;
+}
+
+// make_tree with mem_bytes (SIZE_MAX: one chunk; 8000: the narrow phase's
+// default chunked tree), then `steps` simulation steps in which body B moves:
+// refit_tree and tandem_traversal once with kdop::sequential and once with
+// the kdop::cuda tag (whose device scenes persist between the steps).
+template <size_t K>
+static int run(kdop_ctx* ctx, int n, float pen, float angle, size_t mem_bytes, int steps) {
   Body a, b;
   lattice(a, n);
   lattice(b, n);
-  kdop::Tree<T, K> ta = kdop::make_tree<V, K, T>((size_t)-1, a.mesh, a.X0, a.Y0, a.Z0, kdop::sequential());
-  kdop::Tree<T, K> tb = kdop::make_tree<V, K, T>((size_t)-1, b.mesh, b.X0, b.Y0, b.Z0, kdop::sequential());
+  kdop::Tree<T, K> ta = kdop::make_tree<V, K, T>(mem_bytes, a.mesh, a.X0, a.Y0, a.Z0, kdop::sequential());
+  kdop::Tree<T, K> tb = kdop::make_tree<V, K, T>(mem_bytes, b.mesh, b.X0, b.Y0, b.Z0, kdop::sequential());
+  kdop::Tree<T, K> ta_cuda = ta, tb_cuda = tb;
   MT::quaternion_type qa(1.f, 0.f, 0.f, 0.f);
   float s = std::sin(angle / 2), c = std::cos(angle / 2);
   MT::quaternion_type qb(c, s * 0.267f, s * 0.535f, s * 0.802f);
-  pose(a, qa, V::make(0.f, 0.f, 0.f));
-  pose(b, qb, V::make((float)n - pen, 0.f, 0.f));
-
-  // refit: sequential vs cuda, node volumes bit for bit
-  kdop::Tree<T, K> ta_cuda = ta, tb_cuda = tb;
-  kdop::refit_tree<V, K, T>(ta, a.mesh, a.X, a.Y, a.Z, kdop::sequential());
-  kdop::refit_tree<V, K, T>(tb, b.mesh, b.X, b.Y, b.Z, kdop::sequential());
   kdop::cuda tag(ctx);
-  kdop::refit_tree<V, K, T>(ta_cuda, a.mesh, a.X, a.Y, a.Z, tag);
-  kdop::refit_tree<V, K, T>(tb_cuda, b.mesh, b.X, b.Y, b.Z, tag);
-  int bad = 0;
-  for (int w = 0; w < 2; ++w) {
-    kdop::SubTree<T, K> const& s1 = (w ? tb : ta).branches()[0];
-    kdop::SubTree<T, K> const& s2 = (w ? tb_cuda : ta_cuda).branches()[0];
-    for (size_t i = 0; i < s1.m_nodes.size(); ++i) {
-      if (s1.m_nodes[i].is_undefined()) continue;
-      for (size_t k = 0; k < K / 2; ++k)
-        if (std::memcmp(&s1.m_nodes[i].m_volume(k), &s2.m_nodes[i].m_volume(k), sizeof(geometry::Interval<T>)))
-          ++bad;
-    }
-  }
+  int fails = 0;
+  for (int step = 0; step < steps; ++step) {
+    pose(a, qa, V::make(0.f, 0.f, 0.f));
+    pose(b, qb, V::make((float)n - pen - 0.05f * (float)step, 0.02f * (float)step, 0.f));
+    // refit: sequential vs cuda, every node volume of every level bit for bit
+    kdop::refit_tree<V, K, T>(ta, a.mesh, a.X, a.Y, a.Z, kdop::sequential());
+    kdop::refit_tree<V, K, T>(tb, b.mesh, b.X, b.Y, b.Z, kdop::sequential());
+    kdop::refit_tree<V, K, T>(ta_cuda, a.mesh, a.X, a.Y, a.Z, tag);
+    kdop::refit_tree<V, K, T>(tb_cuda, b.mesh, b.X, b.Y, b.Z, tag);
+    int bad = volume_mismatches<K>(ta, ta_cuda) + volume_mismatches<K>(tb, tb_cuda);
 
-  // traversal + contacts: sequential vs cuda, through the callbacks
-  Rows r_seq, r_cuda;
-  std::vector<kdop::TestPair<V, K, T> > pool_seq, pool_cuda;
-  pool_seq.push_back(kdop::TestPair<V, K, T>(ta, tb, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z, a.surf, b.surf,
-                                             r_seq));
-  pool_cuda.push_back(kdop::TestPair<V, K, T>(ta, tb, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z, a.surf, b.surf,
-                                              r_cuda));
-  kdop::tandem_traversal<V, K, T>(pool_seq, kdop::sequential());
-  kdop::tandem_traversal<V, K, T>(pool_cuda, tag);
-  bool same = r_seq.sorted() == r_cuda.sorted();
-  std::printf("K=%d n=%d: %d volume mismatches, contacts %zu (reference) vs %zu (cuda), %s\n", (int)K, n, bad,
-              r_seq.bits.size() / 7, r_cuda.bits.size() / 7, same ? "identical" : "DIFFERENT");
-  return (bad == 0 && same && !r_seq.bits.empty()) ? 0 : 1;
+    // traversal + contacts: sequential vs cuda, through the callbacks
+    Rows r_seq, r_cuda;
+    std::vector<kdop::TestPair<V, K, T> > pool_seq, pool_cuda;
+    pool_seq.push_back(kdop::TestPair<V, K, T>(ta, tb, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z, a.surf, b.surf,
+                                               r_seq));
+    pool_cuda.push_back(kdop::TestPair<V, K, T>(ta_cuda, tb_cuda, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z,
+                                                a.surf, b.surf, r_cuda));
+    kdop::tandem_traversal<V, K, T>(pool_seq, kdop::sequential());
+    kdop::tandem_traversal<V, K, T>(pool_cuda, tag);
+    bool same = r_seq.sorted() == r_cuda.sorted();
+    std::printf("K=%d n=%d %s (%zu levels, %zu chunks) step %d: %d volume mismatches, contacts %zu (reference) vs "
+                "%zu (cuda), %s\n",
+                (int)K, n, mem_bytes == (size_t)-1 ? "one chunk" : "chunked", ta.number_of_levels(),
+                ta.branches().size(), step, bad, r_seq.bits.size() / 7, r_cuda.bits.size() / 7,
+                same ? "identical" : "DIFFERENT");
+    if (!(bad == 0 && same && !r_seq.bits.empty())) ++fails;
+  }
+  return fails;
 }
 
-int main() {
+static double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Times `steps` narrow-phase steps of two n^3-cell bodies with the default
+// chunked trees (8000 bytes, narrow_object.h:113-128): pose of B, refit_tree
+// of both bodies, tandem_traversal with contacts; once with kdop::sequential
+// and once with the kdop::cuda tag.  Prints milliseconds per step.
+template <size_t K>
+static int time_loop(kdop_ctx* ctx, int n, int steps) {
+  Body a, b;
+  lattice(a, n);
+  lattice(b, n);
+  kdop::Tree<T, K> ta = kdop::make_tree<V, K, T>(8000, a.mesh, a.X0, a.Y0, a.Z0, kdop::sequential());
+  kdop::Tree<T, K> tb = kdop::make_tree<V, K, T>(8000, b.mesh, b.X0, b.Y0, b.Z0, kdop::sequential());
+  MT::quaternion_type qa(1.f, 0.f, 0.f, 0.f), qb(0.9998f, 0.0053f, 0.0107f, 0.016f);
+  pose(a, qa, V::make(0.f, 0.f, 0.f));
+  kdop::cuda tag(ctx);
+  size_t contacts[2] = {0, 0};
+  double ms[2];
+  for (int backend = 0; backend < 2; ++backend) {
+    // one untimed step (the tag's scenes are created in it), then the loop
+    double t0 = 0;
+    for (int step = -1; step < steps; ++step) {
+      if (step == 0) t0 = now_ms();
+      pose(b, qb, V::make((float)n - 0.3f - 0.001f * (float)step, 0.f, 0.f));
+      Rows r;
+      std::vector<kdop::TestPair<V, K, T> > pool;
+      pool.push_back(kdop::TestPair<V, K, T>(ta, tb, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z, a.surf, b.surf, r));
+      if (backend == 0) {
+        kdop::refit_tree<V, K, T>(ta, a.mesh, a.X, a.Y, a.Z, kdop::sequential());
+        kdop::refit_tree<V, K, T>(tb, b.mesh, b.X, b.Y, b.Z, kdop::sequential());
+        kdop::tandem_traversal<V, K, T>(pool, kdop::sequential());
+      } else {
+        kdop::refit_tree<V, K, T>(ta, a.mesh, a.X, a.Y, a.Z, tag);
+        kdop::refit_tree<V, K, T>(tb, b.mesh, b.X, b.Y, b.Z, tag);
+        kdop::tandem_traversal<V, K, T>(pool, tag);
+      }
+      contacts[backend] += r.bits.size() / 7;
+    }
+    ms[backend] = (now_ms() - t0) / steps;
+  }
+  std::printf("loop K=%d n=%d (%zu tets per body, %zu chunks): %d steps, sequential %.3f ms/step, "
+              "kdop::cuda %.3f ms/step, contacts %zu vs %zu\n",
+              (int)K, n, a.mesh.tetrahedron_size(), ta.branches().size(), steps, ms[0], ms[1], contacts[0],
+              contacts[1]);
+  return contacts[0] == contacts[1] && contacts[0] > 0 ? 0 : 1;
+}
+
+int main(int argc, char** argv) {
   kdop_ctx* ctx = 0;
   int rc = kdop_ctx_create(0, &ctx);
   if (rc != KDOP_OK) {
@@ -152,9 +227,22 @@ int main() {
     return 2;
   }
   int fails = 0;
-  fails += run<14>(ctx, 4, 0.3f, 0.05f);
-  fails += run<26>(ctx, 5, 0.2f, 0.08f);
-  fails += run<8>(ctx, 3, 0.4f, 0.03f);
+  if (argc > 1 && std::strcmp(argv[1], "--time") == 0) {
+    int steps = argc > 2 ? std::atoi(argv[2]) : 100;
+    int n = argc > 3 ? std::atoi(argv[3]) : 16;
+    fails += time_loop<8>(ctx, n, steps);
+  } else {
+    const size_t one = (size_t)-1;
+    fails += run<14>(ctx, 4, 0.3f, 0.05f, one, 2);
+    fails += run<26>(ctx, 5, 0.2f, 0.08f, one, 1);
+    fails += run<8>(ctx, 3, 0.4f, 0.03f, one, 1);
+    // the narrow phase's default 8000-byte chunks: several branches, a super
+    // chunk level above them at n = 12 (K = 8: 2 levels)
+    fails += run<8>(ctx, 6, 0.4f, 0.03f, 8000, 3);
+    fails += run<8>(ctx, 12, 0.3f, 0.02f, 8000, 2);
+    fails += run<14>(ctx, 8, 0.3f, 0.04f, 8000, 2);
+  }
+  kdop::cuda_release(ctx);
   kdop_ctx_destroy(ctx);
   std::printf(fails ? "FAIL\n" : "OK\n");
   return fails ? 1 : 0;

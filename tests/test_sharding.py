@@ -73,3 +73,73 @@ def test_two_gloo_ranks_gather_the_unsharded_result(tmp_path, oracle):
     for r in range(world):
         got = np.load(tmp_path / f"rank{r}.npy")
         assert np.array_equal(got, want)
+
+
+def test_config3_keep_builds_the_same_pairs():
+    """config3(keep=...) skips the other pairs' jitter draws without drawing
+    them, so the kept pairs equal the whole scene's."""
+    full = scenes.config3(n_pairs=24, seed=13, max_tets=2e4)
+    keep = [20, 3, 11, 0]
+    part = scenes.config3(n_pairs=24, seed=13, max_tets=2e4, keep=keep)
+    assert np.array_equal(part.extra["pair_ids"], keep)
+    for k, i in enumerate(keep):
+        for s in range(2):
+            a, b = full.meshes[full.pairs[i, s]], part.meshes[part.pairs[k, s]]
+            assert np.array_equal(a.xyz, b.xyz) and np.array_equal(a.tets, b.tets) and np.array_equal(a.surf, b.surf)
+            assert np.array_equal(full.quat[full.pairs[i, s]], part.quat[part.pairs[k, s]])
+            assert np.array_equal(full.pos[full.pairs[i, s]], part.pos[part.pairs[k, s]])
+    tets = np.array([full.meshes[a].n_tets + full.meshes[b].n_tets for a, b in full.pairs])
+    assert np.array_equal(part.extra["pair_tets"], tets)
+
+
+def _bench_rank_main(rank, world, port, out_dir):
+    """One rank of the benchmark's partitioned workload (bench.workload), the
+    oracle standing in for the GPU traversal; rows gathered with global pair
+    indices."""
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root, os.path.join(root, "bvh-tvcg18_b200")]
+    import argparse
+
+    import torch.distributed as dist
+
+    import bench
+    from kdop_b200 import sharding
+    from oracle.pyoracle import Oracle
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        args = argparse.Namespace(workload="config3", pairs=6)
+        sc = bench.workload(args, rank, world)
+        O = Oracle()
+        worlds = [O.rotate(sc.quat[i], sc.pos[i], m.xyz) for i, m in enumerate(sc.meshes)]
+        rows, tpp, _ = O.run_pairs(sc.K, worlds, sc.meshes, sc.pairs, threads=1)
+        allrows = sharding.gather_rows(rows, sc.extra["pair_ids"])
+        np.save(os.path.join(out_dir, f"bench_rank{rank}.npy"), allrows)
+        np.save(os.path.join(out_dir, f"bench_ids{rank}.npy"), sc.extra["pair_ids"])
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_run_the_partitioned_benchmark_workload(tmp_path, oracle):
+    """bench.py's multi-GPU layout on 2 gloo ranks: one workload of 6 pairs
+    per rank x 2, split by estimated cost, every pair on exactly one rank,
+    the gathered rows equal to the unsharded workload's."""
+    world = 2
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_bench_rank_main, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    ids = [np.load(tmp_path / f"bench_ids{r}.npy") for r in range(world)]
+    assert np.array_equal(np.sort(np.concatenate(ids)), np.arange(12))
+    sc = scenes.config3(n_pairs=12)
+    worlds = [oracle.rotate(sc.quat[i], sc.pos[i], m.xyz) for i, m in enumerate(sc.meshes)]
+    rows, _, _ = oracle.run_pairs(sc.K, worlds, sc.meshes, sc.pairs, threads=4)
+    want = rows.astype(np.int64)
+    want = want[np.lexsort((want[:, 2], want[:, 1], want[:, 0]))]
+    for r in range(world):
+        assert np.array_equal(np.load(tmp_path / f"bench_rank{r}.npy"), want)
