@@ -10,9 +10,13 @@ overlap_dop_dop calls, counted exactly as the reference counts them).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
-N > 1 runs under torch.distributed (one rank per GPU); every rank processes
-its own 512-pair batch (weak scaling, no data exchange); the step time is the
-max over ranks.
+N > 1 runs under torch.distributed (one rank per GPU): one workload of
+512 x N pairs (the same seeded generator) is split over the ranks by
+estimated cost (kdop_b200.sharding.partition), so every GPU holds about one
+headline batch (weak scaling) and no data crosses between GPUs on the data
+path; the step time is the max over ranks.  --shard instead splits the
+node-pair tree of the same pairs over the ranks (strong scaling) and
+all-gathers the contact rows to rank 0 over NCCL.
 """
 from __future__ import annotations
 
@@ -561,55 +565,71 @@ def run_cuda(args):
         plain = {"traversal_ms": plain_ms, "tests_per_s": state_tests / (plain_ms * 1e-3),
                  "batched_speedup": plain_ms / trav_ms, "launch_shape": best[1], "opts": best[2]}
 
-    # e2e: through the public API with host buffers; per step the world
-    # positions of all meshes go host->device (pinned) and the contacts and
-    # counters come back device->host
-    # the world positions of the posed meshes, as the library's pose refit
-    # computes them (read back once, outside the timed region)
+    # e2e: through the public API with host buffers, two forms.  Rigid bodies
+    # (the reference's narrow_update_kdop_bvh.h:146-171: pose, then refit):
+    # per step the poses of all meshes and the pair list go host->device from
+    # pinned memory (kdop_set_poses + kdop_refit(POSE)), then traversal and
+    # contacts, and the contact rows and counters come back device->host.
+    # Deformable bodies: the world positions of all meshes go host->device
+    # instead (kdop_set_vertices + kdop_refit(VERTICES), 12 bytes a vertex).
     ds.set_poses(sc.quat, sc.pos)
     ds.refit(kd.REFIT_POSE)
+    # the world positions of the posed meshes, as the library's pose refit
+    # computes them (read back once, outside the timed region)
     world = ds.read_vertices()
     h_xyz = torch.empty((world.shape[0], 3), dtype=torch.float32, pin_memory=True)
     h_xyz.numpy()[:] = world
+    h_quat = torch.empty((len(sc.quat), 4), dtype=torch.float32, pin_memory=True)
+    h_quat.numpy()[:] = sc.quat
+    h_pos = torch.empty((len(sc.pos), 3), dtype=torch.float32, pin_memory=True)
+    h_pos.numpy()[:] = sc.pos
     h_pairs = torch.empty((len(sc.pairs), 2), dtype=torch.int32, pin_memory=True)
     h_pairs.numpy()[:] = sc.pairs.astype(np.int32)
     n_cont_cap = ds.stats().contact_capacity
     h_cont = torch.empty((n_cont_cap * 8,), dtype=torch.float32, pin_memory=True)
     import ctypes
 
-    def e2e_step():
-        ds.set_vertices(h_xyz.numpy())
-        ds.refit(kd.REFIT_VERTICES)
+    def e2e_step(vertices: bool):
+        if vertices:
+            ds.set_vertices(h_xyz.numpy())
+            ds.refit(kd.REFIT_VERTICES)
+        else:
+            ds.set_poses(h_quat.numpy(), h_pos.numpy())
+            ds.refit(kd.REFIT_POSE)
         ds.traverse(h_pairs.numpy().view(np.uint32), opts)
         ds.contacts()
         s = ds.stats()
-        n = C_n = ctypes.c_int64()
+        n = ctypes.c_int64()
         ds.ctx._check(ds.lib.kdop_read_contacts(ds.h, ctypes.c_void_p(h_cont.data_ptr()), n_cont_cap,
-                                                ctypes.byref(C_n)))
+                                                ctypes.byref(n)))
         return s, n.value
 
-    for _ in range(2):
-        e2e_step()
-    ctx.synchronize()
-    dist.barrier()
-    w0 = time.perf_counter()
-    b0 = torch.cuda.Event(enable_timing=True)
-    b1 = torch.cuda.Event(enable_timing=True)
-    b0.record(stream)
-    ncont = 0
-    for _ in range(args.e2e_steps):
-        s, ncont = e2e_step()
-    b1.record(stream)
-    b1.synchronize()
-    e2e_ms = max(b0.elapsed_time(b1), (time.perf_counter() - w0) * 1e3) / args.e2e_steps
-    if not deforming:
-        assert s.n_tests == tests_per_step
-    e2e_ms_max = dist.max(e2e_ms)
-    # the end-to-end step traverses the rigidly posed meshes (config 4: without
-    # its deformation), so it is rated by its own test count
-    e2e_value = dist.sum(float(s.n_tests)) / (e2e_ms_max * 1e-3)
-    h2d = world.nbytes + sc.pairs.nbytes
+    def e2e_time(vertices: bool):
+        for _ in range(2):
+            e2e_step(vertices)
+        ctx.synchronize()
+        dist.barrier()
+        w0 = time.perf_counter()
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(args.e2e_steps):
+            s, ncont = e2e_step(vertices)
+        b1.record(stream)
+        b1.synchronize()
+        ms = max(b0.elapsed_time(b1), (time.perf_counter() - w0) * 1e3) / args.e2e_steps
+        if not deforming:
+            assert s.n_tests == tests_per_step
+        ms_max = dist.max(ms)
+        # the end-to-end step traverses the rigidly posed meshes (config 4:
+        # without its deformation), so it is rated by its own test count
+        return dist.sum(float(s.n_tests)) / (ms_max * 1e-3), ms_max, ncont
+
+    e2e_value, e2e_ms_max, ncont = e2e_time(False)
+    h2d = h_quat.numpy().nbytes + h_pos.numpy().nbytes + sc.pairs.nbytes
     d2h = ncont * 32 + 128
+    e2e_v_value, e2e_v_ms, ncont_v = e2e_time(True)
+    h2d_v = world.nbytes + sc.pairs.nbytes
 
     # CPU baseline: the reference's own CPU path, one thread, bounded sample
     cpu = None
@@ -666,7 +686,13 @@ def run_cuda(args):
             "plain": plain,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-                    "ms_per_step": e2e_ms_max},
+                    "ms_per_step": e2e_ms_max,
+                    "inputs": "per step: poses of every mesh and the pair list H2D (kdop_set_poses, pinned), "
+                              "contact rows and counters D2H"},
+            "e2e_vertices": {"value": e2e_v_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d_v),
+                             "d2h_bytes_per_step": int(ncont_v * 32 + 128), "ms_per_step": e2e_v_ms,
+                             "inputs": "per step: world positions of every vertex and the pair list H2D "
+                                       "(kdop_set_vertices, pinned), contact rows and counters D2H"},
             "gpu_launches": int(launches_timed),
             "clocks": clk,
         }
