@@ -196,18 +196,18 @@ def shape_key(opts) -> str:
                                             "wave_pairs", "smem_carveout"))
 
 
-def traverse_dram_capture(workload: str, opts):
+def traverse_dram_capture(workload: str, pairs: int, opts):
     """DRAM bytes per node-pair test and L1 data-pipe use of the traversal
     launch, from the ncu capture of the same launch shape on the same
-    workload family (profiles/traverse_dram.json); None when no capture of
-    this shape exists, so that no traffic is quoted for a shape nobody
-    measured."""
+    workload (profiles/traverse_dram.json, keyed by workload and pair count);
+    None when no capture of this launch exists, so that no traffic is quoted
+    for a launch nobody measured."""
     path = os.path.join(ROOT, "profiles", "traverse_dram.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
-    return d.get("captures", {}).get(workload, {}).get(shape_key(opts))
+    return d.get("captures", {}).get(f"{workload}:{pairs}", {}).get(shape_key(opts))
 
 
 def workload(args, rank: int = 0, world: int = 1):
@@ -529,10 +529,10 @@ def run_cuda(args):
     alg_bytes = state_tests * 2 * node_bytes
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (trav_ms * 1e-3) / 1e9
-    # DRAM bytes of this launch: the capture of the same launch shape on a
-    # smaller case of the same generator, scaled by node-pair tests (the
-    # launch's DRAM traffic grows with its tests)
-    cap = traverse_dram_capture(args.workload, opts)
+    # DRAM bytes of this launch: the ncu capture of the same launch (shape
+    # and workload), per node-pair test
+    cap = (traverse_dram_capture(args.workload, int(sc.extra.get("pairs_total", len(sc.pairs))), opts)
+           if dist.world == 1 else None)
     traffic = cap["dram_bytes_per_test"] * state_tests if cap else None
 
     # plain: one traversal launch per mesh pair, same trees and descent rule;
@@ -681,6 +681,7 @@ def run_cuda(args):
                          "dram_gbs": (traffic / (trav_ms * 1e-3) / 1e9) if traffic else None,
                          "dram_frac": (traffic / (trav_ms * 1e-3) / 1e9 / peak) if traffic else None,
                          "l1_lsu_pct": cap["l1_lsu_pct"] if cap else None,
+                         "l1_lsu_pct_source": cap.get("l1_lsu_pct_source") if cap else None,
                          "traffic_source": (cap["source"] if cap else
                                             "no ncu capture of this launch shape: traffic not quoted")},
             "plain": plain,

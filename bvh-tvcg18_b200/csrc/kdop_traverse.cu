@@ -173,6 +173,7 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
   const int lane = threadIdx.x & 31;
   const int wib = threadIdx.x >> 5;
   const int ge = lane / Q, gq = lane % Q;  // entry and chunk lane of this lane
+  const float4* __restrict__ nodes_q = a.nodes + 2 * gq;  // chunk gq of twin 0
   const unsigned lt_mask = (1u << lane) - 1u;
   const int CAP = a.stack_cap;
   const int MASK = CAP - 1;
@@ -221,8 +222,8 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
     unsigned q_h = 0, q_t = 0;
     ++step;
     if ((step & 1023u) == 0u) fold_counts();
-    // warp-uniform: poll the queue counters on every 4th step with work
-    const bool polled = top - bot >= 2 && (step & 3u) == 0u;
+    // warp-uniform: poll the queue counters on every 16th step with work
+    const bool polled = top - bot >= 2 && (step & 15u) == 0u;
     if (lane == 0 && polled) {
       q_h = ld_volatile(&ctl->q_head);
       q_t = ld_volatile(&ctl->q_tail);
@@ -357,16 +358,16 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
           eab[b] = sAB[at];
           ep[b] = mixed ? sP[at] : curP;
         }
-        const int64_t ta = (int64_t)((eab[b].x & NODE_MASK) >> 1) * (2 * NW);
-        const int64_t tb = (int64_t)((eab[b].y & NODE_MASK) >> 1) * (2 * NW);
+        const float4* pa = nodes_q + (size_t)((eab[b].x & NODE_MASK) >> 1) * (2 * NW);
+        const float4* pb = nodes_q + (size_t)((eab[b].y & NODE_MASK) >> 1) * (2 * NW);
 #pragma unroll
         for (int r = 0; r < C; ++r) {
           const int j = gq + Q * r;
           // a lane without an entry (i >= n) loads the record of node 0's
           // twin and its verdicts are never used: no zero fill
           if (j < NW) {
-            ldg256(a.nodes + ta + 2 * j, A0[b][r], A1[b][r]);
-            ldg256(a.nodes + tb + 2 * j, B0[b][r], B1[b][r]);
+            ldg256(pa + 2 * Q * r, A0[b][r], A1[b][r]);
+            ldg256(pb + 2 * Q * r, B0[b][r], B1[b][r]);
           }
         }
       }
