@@ -60,6 +60,7 @@ struct TravArgs {
   unsigned n_meshes;
   const uint32_t* __restrict__ order;  // root pair i -> pair index (NULL: identity)
   const uint4* __restrict__ entries;   // when set: initial work = these deque entries (A, B, pair)
+  unsigned poll_mask;  // queue counters polled on steps with (step & poll_mask) == 0
 };
 
 // Device buffers one traversal works in: pairs (input), candidates (output),
@@ -222,8 +223,9 @@ __global__ void __launch_bounds__(512, (C * S >= 4) ? 1 : 2) traverse_kernel(Tra
     unsigned q_h = 0, q_t = 0;
     ++step;
     if ((step & 1023u) == 0u) fold_counts();
-    // warp-uniform: poll the queue counters on every 16th step with work
-    const bool polled = top - bot >= 2 && (step & 15u) == 0u;
+    // warp-uniform: poll the queue counters on every (poll_mask + 1)-th step
+    // with work
+    const bool polled = top - bot >= 2 && (step & a.poll_mask) == 0u;
     if (lane == 0 && polled) {
       q_h = ld_volatile(&ctl->q_head);
       q_t = ld_volatile(&ctl->q_tail);
@@ -650,6 +652,12 @@ static cudaError_t traverse_impl(kdop_scene* s, int64_t n_pairs, const TravBuffe
   a.donate_min = p.donate_min;
   a.surface_filter = p.surface_filter;
   a.timeout_ns = p.timeout_ns;
+  // Donations reach waiting warps only through polls.  A batched launch keeps
+  // most warps busy with root pairs and polls every 16th step (config 3: 10.49
+  // ms vs 10.65 ms every 4th step); a one-pair launch leaves most warps
+  // waiting for donations and polls every 4th step (config 3, one launch per
+  // pair: 88 ms vs 103 ms every 16th).
+  a.poll_mask = plain ? 3u : 15u;
   if (b.entries) {
     // seeded by a frontier: its tests and leaf pairs are in the totals already
     trav_init_kernel<<<1, 32, 0, st>>>(b.ctl, (unsigned)n_pairs, 0u, 0, p.stuck_work);
