@@ -9,6 +9,8 @@ checked-in file stays a few kilobytes:
   config 2  one pair of 64^3-cell jittered lattices, k = 26
   config 3  512 uneven pairs (1k-200k tets), k = 14
   config 5  256 touching pairs of 20^3-cell lattices, k = 14
+  config 4  64 pairs of 40^3-cell lattices at their initial rigid poses
+            (the deforming benchmark's meshes before any step), k = 18
 
 Per workload: node-pair tests (total and per pair), the number of candidate
 tet pairs (leaf pairs reaching contact generation) with the sha256 of their
@@ -68,6 +70,7 @@ WORKLOADS = {
     "config2": lambda: scenes.config2(),
     "config3": lambda: scenes.config3(),
     "config5": lambda: scenes.config5(),
+    "config4": lambda: scenes.config4(),
 }
 
 

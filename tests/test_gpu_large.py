@@ -153,6 +153,17 @@ def test_config4_graph_steps_match_oracle(ctx, oracle):
     ds.graph_release()
 
 
+def test_config4_meshes_at_rest_poses_k18(ctx, golden_large):
+    """Config 4's 64 pairs of 384,000-tet meshes at their initial rigid poses
+    (before any deforming step), k = 18: node-pair tests, candidates and
+    FP32 contacts equal the reference's own."""
+    sc = scenes.config4()
+    ds = device_scene(ctx, sc)
+    st = ds.traverse_sync(sc.pairs, contacts=True)
+    check_reference(ds, st, golden_large["config4"])
+    ds.close()
+
+
 def oracle_step(oracle, sc, world, v_off):
     """Candidates (pair, a, b) and node-pair tests of the oracle on the given
     world positions, trees built on the rest positions."""

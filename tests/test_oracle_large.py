@@ -5,8 +5,9 @@ by tests/golden/make_golden_large.py from the compiled reference).
 This closes the chain reference -> restatement at the sizes the benchmark
 runs: node-pair tests per pair, the canonical candidate list and the FP32
 contact rows of config 2 (one pair of 1.57 M-tet meshes, k = 26), config 3
-(512 uneven pairs, k = 14) and config 5 (256 touching pairs, 3.5 M contacts,
-k = 14).  The GPU tests compare the CUDA library with the same digests.
+(512 uneven pairs, k = 14), config 5 (256 touching pairs, 3.5 M contacts,
+k = 14) and config 4's 64 pairs of 384 k-tet meshes at their initial rigid
+poses (k = 18).  The GPU tests compare the CUDA library with the same digests.
 """
 import os
 
@@ -16,7 +17,8 @@ import pytest
 from conftest import canonical_candidates, canonical_contacts, digest
 from kdop_b200 import scenes
 
-WORKLOADS = {"config2": scenes.config2, "config3": scenes.config3, "config5": scenes.config5}
+WORKLOADS = {"config2": scenes.config2, "config3": scenes.config3, "config5": scenes.config5,
+             "config4": scenes.config4}
 
 
 def oracle_summary(oracle, sc, contacts=True):
