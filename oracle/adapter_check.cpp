@@ -170,6 +170,55 @@ static int run(kdop_ctx* ctx, int n, float pen, float angle, size_t mem_bytes, i
   return fails;
 }
 
+// Pools whose mesh sets change between steps: bodies A, B, C (chunked
+// trees); the pool holds {A-B, A-C} (A shared: one device mesh for it), then
+// {A-B}, then {A-B, A-C} again (the tag's cached scene of the first pool is
+// reused).  Each pair's callback must receive the sequential back-end's
+// contacts.
+template <size_t K>
+static int run_pools(kdop_ctx* ctx, int n) {
+  Body a, b, c;
+  lattice(a, n);
+  lattice(b, n);
+  lattice(c, n);
+  kdop::Tree<T, K> ta = kdop::make_tree<V, K, T>(8000, a.mesh, a.X0, a.Y0, a.Z0, kdop::sequential());
+  kdop::Tree<T, K> tb = kdop::make_tree<V, K, T>(8000, b.mesh, b.X0, b.Y0, b.Z0, kdop::sequential());
+  kdop::Tree<T, K> tc = kdop::make_tree<V, K, T>(8000, c.mesh, c.X0, c.Y0, c.Z0, kdop::sequential());
+  MT::quaternion_type q0(1.f, 0.f, 0.f, 0.f), qb(0.9998f, 0.0053f, 0.0107f, 0.016f),
+      qc(0.9997f, -0.012f, 0.0081f, 0.02f);
+  kdop::cuda tag(ctx);
+  int fails = 0;
+  const int pools[3] = {2, 1, 2};
+  for (int step = 0; step < 3; ++step) {
+    pose(a, q0, V::make(0.f, 0.f, 0.f));
+    pose(b, qb, V::make((float)n - 0.3f - 0.05f * (float)step, 0.f, 0.f));
+    pose(c, qc, V::make(0.f, (float)n - 0.25f, 0.02f * (float)step));
+    kdop::refit_tree<V, K, T>(ta, a.mesh, a.X, a.Y, a.Z, kdop::sequential());
+    kdop::refit_tree<V, K, T>(tb, b.mesh, b.X, b.Y, b.Z, kdop::sequential());
+    kdop::refit_tree<V, K, T>(tc, c.mesh, c.X, c.Y, c.Z, kdop::sequential());
+    Rows seq[2], gpu[2];
+    std::vector<kdop::TestPair<V, K, T> > ps, pg;
+    ps.push_back(kdop::TestPair<V, K, T>(ta, tb, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z, a.surf, b.surf, seq[0]));
+    pg.push_back(kdop::TestPair<V, K, T>(ta, tb, a.mesh, b.mesh, a.X, b.X, a.Y, b.Y, a.Z, b.Z, a.surf, b.surf, gpu[0]));
+    if (pools[step] == 2) {
+      ps.push_back(kdop::TestPair<V, K, T>(ta, tc, a.mesh, c.mesh, a.X, c.X, a.Y, c.Y, a.Z, c.Z, a.surf, c.surf,
+                                           seq[1]));
+      pg.push_back(kdop::TestPair<V, K, T>(ta, tc, a.mesh, c.mesh, a.X, c.X, a.Y, c.Y, a.Z, c.Z, a.surf, c.surf,
+                                           gpu[1]));
+    }
+    kdop::tandem_traversal<V, K, T>(ps, kdop::sequential());
+    kdop::tandem_traversal<V, K, T>(pg, tag);
+    for (int i = 0; i < pools[step]; ++i) {
+      bool same = seq[i].sorted() == gpu[i].sorted() && !seq[i].bits.empty();
+      std::printf("K=%d n=%d pool of %d pairs, step %d, pair %d: contacts %zu (reference) vs %zu (cuda), %s\n",
+                  (int)K, n, pools[step], step, i, seq[i].bits.size() / 7, gpu[i].bits.size() / 7,
+                  same ? "identical" : "DIFFERENT");
+      if (!same) ++fails;
+    }
+  }
+  return fails;
+}
+
 static double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
@@ -241,6 +290,7 @@ int main(int argc, char** argv) {
     fails += run<8>(ctx, 6, 0.4f, 0.03f, 8000, 3);
     fails += run<8>(ctx, 12, 0.3f, 0.02f, 8000, 2);
     fails += run<14>(ctx, 8, 0.3f, 0.04f, 8000, 2);
+    fails += run_pools<8>(ctx, 6);
   }
   kdop::cuda_release(ctx);
   kdop_ctx_destroy(ctx);

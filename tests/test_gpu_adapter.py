@@ -4,9 +4,10 @@ make_tree / refit_tree / tandem_traversal once with kdop::sequential and once
 with the kdop::cuda tag on the same meshes, over several simulation steps
 (the tag's device scenes persist between them), for one-chunk trees (K = 8,
 14, 26) and the narrow phase's default 8000-byte chunked trees (K = 8, 14;
-branches and a super-chunk level), and exits 0 when every node volume of
-every chunk level and the root kDOP are bit-identical and the callbacks
-received the same contacts."""
+branches and a super-chunk level), and for pools whose mesh sets change
+between steps (one body shared by two pairs; a cached scene reused), and
+exits 0 when every node volume of every chunk level and the root kDOP are
+bit-identical and the callbacks received the same contacts."""
 import os
 import subprocess
 
