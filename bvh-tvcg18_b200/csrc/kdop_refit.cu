@@ -92,15 +92,54 @@ __global__ void __launch_bounds__(256) refit_level_kernel(float4* nodes, int64_t
   refit_node<K, true>(nodes, begin + t, tets, vs, dt);
 }
 
-// Levels [0, last] of the forest, deepest first, by a single block (plain
-// loads: the block reads records it wrote itself).
+// Depths [0, top] of every tree: one block per tree.  The block lists its
+// tree's nodes of those depths top-down from the root (children from the
+// topology words), then refits them bottom-up, a block barrier per depth
+// (plain loads: the block reads records it wrote itself; the children of
+// depth `top` were refitted by the level launches before it).  One launch
+// replaces the per-level launches of the forest's small top levels, each of
+// which was bound by launch and load latency.  The padding node that may end
+// the root level (a copy of the first root's topology) is refitted by the
+// block of the tree rooted at node 0.
+constexpr int kTopDepth = 10;
+constexpr int kTopNodes = 2 << kTopDepth;  // >= 2^(kTopDepth + 1) - 1 nodes of a tree's top
+
 template <int K>
-__global__ void __launch_bounds__(1024) refit_tail_kernel(float4* nodes, const int64_t* __restrict__ level_off,
-                                                          int last, const uint4* __restrict__ tets,
-                                                          VertexSource vs, DirTable dt) {
-  for (int d = last; d >= 0; --d) {
-    for (int64_t n = level_off[d] + threadIdx.x; n < level_off[d + 1]; n += blockDim.x)
-      refit_node<K, false>(nodes, n, tets, vs, dt);
+__global__ void __launch_bounds__(256) refit_top_kernel(float4* nodes, const uint32_t* __restrict__ root, int top,
+                                                        uint32_t pad_node, const uint4* __restrict__ tets,
+                                                        VertexSource vs, DirTable dt) {
+  using L = NodeLayout<K>;
+  __shared__ uint32_t ids[kTopNodes];
+  __shared__ int lev[kTopDepth + 2];  // nodes of depth d: ids[lev[d] .. lev[d + 1])
+  __shared__ int fill;
+  const uint32_t r = root[blockIdx.x];
+  if (r == NO_NODE) return;  // empty mesh: the whole block leaves
+  if (threadIdx.x == 0) {
+    ids[0] = r;
+    lev[0] = 0;
+    lev[1] = 1;
+    fill = 1;
+  }
+  __syncthreads();
+  for (int d = 0; d < top; ++d) {
+    const int b = lev[d], e = lev[d + 1];
+    for (int i = b + (int)threadIdx.x; i < e; i += blockDim.x) {
+      const uint32_t w0 = L::word0(__ldg(nodes + L::at(ids[i], L::TOPO_CHUNK)));
+      if (!(w0 & LEAF_BIT)) {
+        const int at = atomicAdd(&fill, 2);
+        ids[at] = w0 & NODE_MASK;
+        ids[at + 1] = (w0 & NODE_MASK) + 1u;
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) lev[d + 2] = fill;
+    __syncthreads();
+  }
+  for (int d = top; d >= 0; --d) {
+    for (int i = lev[d] + (int)threadIdx.x; i < lev[d + 1]; i += blockDim.x)
+      refit_node<K, false>(nodes, ids[i], tets, vs, dt);
+    if (d == 0 && r == 0u && pad_node != NO_NODE && threadIdx.x == blockDim.x - 1)
+      refit_node<K, false>(nodes, pad_node, tets, vs, dt);
     __syncthreads();
   }
 }
@@ -211,11 +250,6 @@ static VertexSource vertex_source(kdop_scene* s, int mode) {
   return vs;
 }
 
-// Device copy of the level offsets for the tail kernel (lives in the scene's
-// root_dev allocation after the per-mesh roots).
-static const int64_t* level_off_dev(kdop_scene* s) {
-  return reinterpret_cast<const int64_t*>(s->root_dev + ((s->n_meshes + 1) & ~1));
-}
 
 template <int K>
 static cudaError_t refit_impl(kdop_scene* s, int mode) {
@@ -228,26 +262,25 @@ static cudaError_t refit_impl(kdop_scene* s, int mode) {
     vs = vertex_source(s, KDOP_REFIT_VERTICES);
     vs.world = s->posed;
   }
-  const int64_t small = 4096;  // nodes of a level refitted by the single-block kernel
   int levels = (int)s->level_off.size() - 1;
   if (levels <= 0) return cudaSuccess;
-  int tail = -1;  // levels [0, tail] go to the single-block kernel
-  for (int d = 0; d < levels; ++d) {
-    if (s->level_off[d + 1] - s->level_off[d] <= small)
-      tail = d;
-    else
-      break;
-  }
-  for (int d = levels - 1; d > tail; --d) {
+  // depths [0, top] of every tree in one launch (a block per tree), the
+  // deeper levels one launch each, deepest first
+  const int top = std::min(kTopDepth, levels - 1);
+  for (int d = levels - 1; d > top; --d) {
     int64_t b = s->level_off[d], n = s->level_off[d + 1] - b;
     unsigned grid = (unsigned)((n + 255) / 256);
     refit_level_kernel<K><<<grid, 256, 0, s->ctx->stream>>>(s->nodes, b, n, s->tets, vs, s->dirs);
     s->ctx->launches++;
   }
-  if (tail >= 0) {
-    refit_tail_kernel<K><<<1, 1024, 0, s->ctx->stream>>>(s->nodes, level_off_dev(s), tail, s->tets, vs, s->dirs);
-    s->ctx->launches++;
-  }
+  // the root level holds one padding node after the real roots when their
+  // count is odd
+  int64_t n_roots = 0;
+  for (int m = 0; m < s->n_meshes; ++m) n_roots += (s->t_off[m + 1] > s->t_off[m]) ? 1 : 0;
+  const uint32_t pad = (s->level_off[1] - s->level_off[0] > n_roots) ? (uint32_t)(s->level_off[1] - 1) : NO_NODE;
+  refit_top_kernel<K><<<(unsigned)s->n_meshes, 256, 0, s->ctx->stream>>>(s->nodes, s->root_dev, top, pad, s->tets,
+                                                                         vs, s->dirs);
+  s->ctx->launches++;
   return cudaGetLastError();
 }
 
