@@ -432,8 +432,7 @@ int kdop_scene_create_ex(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_des
     SC_TRY(dalloc(s, &s->tets, nt));
     SC_TRY(dalloc(s, &s->surf, nt));
     SC_TRY(dalloc(s, &s->nodes, s->nn * s->NW));
-    size_t root_words = (size_t)((n_meshes + 1) & ~1);
-    size_t root_bytes = root_words * 4 + s->level_off.size() * 8;
+    size_t root_bytes = (size_t)n_meshes * 4;
     SC_TRY(cudaMalloc((void**)&s->root_dev, std::max<size_t>(root_bytes, 8)));
     s->device_bytes += (int64_t)root_bytes;
     SC_TRY(dalloc(s, &s->quat, n_meshes));
@@ -450,7 +449,6 @@ int kdop_scene_create_ex(kdop_ctx* ctx, int K, int n_meshes, const kdop_mesh_des
     SC_TRY(cudaMemcpyAsync(s->surf, surf.data(), (size_t)nt, cudaMemcpyHostToDevice, st));
     std::vector<uint8_t> rbuf(std::max<size_t>(root_bytes, 8), 0);
     if (n_meshes) std::memcpy(rbuf.data(), s->root.data(), (size_t)n_meshes * 4);
-    if (!s->level_off.empty()) std::memcpy(rbuf.data() + root_words * 4, s->level_off.data(), s->level_off.size() * 8);
     SC_TRY(cudaMemcpyAsync(s->root_dev, rbuf.data(), root_bytes, cudaMemcpyHostToDevice, st));
     std::vector<float4> q((size_t)std::max(n_meshes, 1), make_float4(1.f, 0.f, 0.f, 0.f));
     std::vector<float4> z((size_t)std::max(n_meshes, 1), make_float4(0.f, 0.f, 0.f, 0.f));

@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(256) refit_level_kernel(float4* nodes, int64_t
 // which was bound by launch and load latency.  The padding node that may end
 // the root level (a copy of the first root's topology) is refitted by the
 // block of the tree rooted at node 0.
-constexpr int kTopDepth = 10;
+constexpr int kTopDepth = 6;
 constexpr int kTopNodes = 2 << kTopDepth;  // >= 2^(kTopDepth + 1) - 1 nodes of a tree's top
 
 template <int K>
