@@ -113,7 +113,7 @@ __device__ __forceinline__ bool node_overlap(const float4* __restrict__ nodes, u
 }
 
 // Waiting warps from which on every deque with work donates (tail mode).
-constexpr int kTailWaiting = 64;
+constexpr int kTailWaiting = 512;
 
 // Warp total and exclusive prefix of per-lane counts below 2^BITS, one
 // ballot per bit.
