@@ -330,6 +330,7 @@ def run_cuda_sharded(args):
     import torch
 
     import kdop_b200 as kd
+    from kdop_b200 import sharding
 
     dist = Dist("nccl")
     torch.cuda.set_device(dist.local)
@@ -359,21 +360,7 @@ def run_cuda_sharded(args):
         st = ds.stats()
         n = ds.read_contacts_into(mine)
         with torch.cuda.stream(stream):
-            counts = torch.tensor([n], dtype=torch.int64, device="cuda")
-            if dist.pg:
-                all_counts = [torch.empty_like(counts) for _ in range(dist.world)]
-                dist.pg.all_gather(all_counts, counts)
-                dist.pg.all_gather(gathered, mine)
-                cnt = [int(c.item()) for c in all_counts]
-            else:
-                gathered[0].copy_(mine)
-                cnt = [n]
-            if dist.rank == 0:
-                off = 0
-                for r, c in enumerate(cnt):
-                    if c:
-                        host_rows[off: off + c * row_bytes].copy_(gathered[r][: c * row_bytes], non_blocking=True)
-                    off += c * row_bytes
+            cnt = sharding.gather_row_buffers(mine, n, row_bytes, gathered, host_rows, dist.rank)
             stream.synchronize()
         return st.n_tests, sum(cnt)
 

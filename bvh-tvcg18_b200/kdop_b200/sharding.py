@@ -56,3 +56,33 @@ def gather_rows(rows: np.ndarray, global_pair_ids: np.ndarray, group=None) -> np
     if len(out):
         out = out[np.lexsort((out[:, 2], out[:, 1], out[:, 0]))]
     return out
+
+
+def gather_row_buffers(mine, n_rows: int, row_bytes: int, gathered, out, rank: int) -> List[int]:
+    """The exchange step of a traversal split over ranks (kdop_traverse_shard):
+    every rank's first n_rows rows (row_bytes bytes each) of `mine`, a byte
+    tensor of the same fixed capacity on every rank, reach rank 0 packed in
+    rank order into `out`.  The row counts are all-gathered first, then the
+    fixed-size buffers into `gathered` (one tensor like `mine` per rank);
+    works on CUDA tensors over NCCL and on CPU tensors over gloo.  Returns the
+    per-rank row counts (on every rank)."""
+    import torch
+    import torch.distributed as dist
+
+    world = len(gathered)
+    if world > 1:
+        counts = torch.tensor([n_rows], dtype=torch.int64, device=mine.device)
+        all_counts = [torch.empty_like(counts) for _ in range(world)]
+        dist.all_gather(all_counts, counts)
+        dist.all_gather(gathered, mine)
+        cnt = [int(c.item()) for c in all_counts]
+    else:
+        gathered[0].copy_(mine)
+        cnt = [int(n_rows)]
+    if rank == 0:
+        off = 0
+        for r, c in enumerate(cnt):
+            if c:
+                out[off: off + c * row_bytes].copy_(gathered[r][: c * row_bytes], non_blocking=True)
+            off += c * row_bytes
+    return cnt

@@ -143,3 +143,52 @@ def test_two_gloo_ranks_run_the_partitioned_benchmark_workload(tmp_path, oracle)
     want = want[np.lexsort((want[:, 2], want[:, 1], want[:, 0]))]
     for r in range(world):
         assert np.array_equal(np.load(tmp_path / f"bench_rank{r}.npy"), want)
+
+
+def _exchange_rank_main(rank, world, port, out_dir):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [root, os.path.join(root, "bvh-tvcg18_b200")]
+    import torch
+    import torch.distributed as dist
+
+    from kdop_b200 import sharding
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    try:
+        row_bytes, cap = 32, 16
+        n = [5, 0, 11][rank]
+        mine = torch.zeros(cap * row_bytes, dtype=torch.uint8)
+        for i in range(n):  # row i of rank r: bytes (r, i, 7, 7, ...)
+            mine[i * row_bytes: (i + 1) * row_bytes] = 7
+            mine[i * row_bytes] = rank
+            mine[i * row_bytes + 1] = i
+        gathered = [torch.empty_like(mine) for _ in range(world)]
+        out = torch.zeros(cap * row_bytes * world, dtype=torch.uint8)
+        cnt = sharding.gather_row_buffers(mine, n, row_bytes, gathered, out, rank)
+        np.save(os.path.join(out_dir, f"ex_cnt{rank}.npy"), np.array(cnt))
+        if rank == 0:
+            np.save(os.path.join(out_dir, "ex_out.npy"), out.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_three_gloo_ranks_exchange_sharded_rows(tmp_path):
+    """The exchange step of the sharded traversal (bench.py --shard): each
+    rank's variable number of fixed-size rows reaches rank 0 packed in rank
+    order; every rank learns every rank's count."""
+    world = 3
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    procs = [ctx.Process(target=_exchange_rank_main, args=(r, world, port, str(tmp_path))) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for r in range(world):
+        assert np.load(tmp_path / f"ex_cnt{r}.npy").tolist() == [5, 0, 11]
+    out = np.load(tmp_path / "ex_out.npy").reshape(-1, 32)
+    want = [(0, i) for i in range(5)] + [(2, i) for i in range(11)]
+    assert [(int(a), int(b)) for a, b in out[:16, :2]] == want
+    assert (out[:16, 2:] == 7).all() and (out[16:] == 0).all()
